@@ -1,0 +1,150 @@
+// fk_device.cuh -- device-side Fenton-Karma model for sm_100a.
+//
+// Data layout in HBM (every state, adjoint state and trajectory slot):
+//   three planes u, v, w of a padded grid, plane = rows_alloc * ld doubles,
+//   logical cell (i, j) at offset (i + HALO) * ld + (j + HALO);
+//   a ring of HALO NaN cells surrounds the grid and holes hold NaN.
+// With a NaN ring the reference's edge rule (mirror the inner neighbour,
+// src/cuda/fk_forward_Et_mono_PARAMETERS.cu:319-361) and its hole rule (a NaN
+// neighbour is replaced by the opposite one, :348-358) are the same rule, and
+// the adjoint stencil's off-grid and hole cases coincide too, so the kernels
+// have no boundary branches and tile loads never leave the allocation.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fkadj {
+
+constexpr int HALO = 4;
+
+// Model constants as the kernels use them: reciprocals replace the divisions
+// by constant time scales of the reference's F_ion / jacT (cu-F:29-45,
+// cu-G:1160-1184); this moves results by at most an ulp per operation.
+struct DevModel {
+    double u_c, u_v, ksm, k_fk, u_csi;
+    double r_tau_d, r_tau_0, r_tau_r, r_2tau_si;
+    double tau_v1m, tau_v2m, r_tau_vp, r_tau_wm, r_tau_wp;
+    double dv12;  // tau_v2_minus - tau_v1_minus
+    double cu, cv, cw;  // D / h^2
+    double dt;
+};
+
+struct DevGrid {
+    int nrows, ncols, ld, rows_alloc;
+    long long plane;  // doubles per field plane
+};
+
+// Ionic currents (formula of cu-F:29-45).
+__device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, double w,
+                                       double& ud, double& vd, double& wd) {
+    const double tc = tanh(P.ksm * (u - P.u_c));
+    const double tv = tanh(P.ksm * (u - P.u_v));
+    const double ts = tanh(P.k_fk * (u - P.u_csi));
+    const double p = 0.5 * (1.0 + tc);
+    const double q = 0.5 * (1.0 + tv);
+    const double j_fi = -v * p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
+    const double j_so = u * (1.0 - p) * P.r_tau_0 + p * P.r_tau_r;
+    const double tvm = q * P.tau_v1m + (1.0 - q) * P.tau_v2m;
+    const double j_si = -w * (1.0 + ts) * P.r_2tau_si;
+    ud = -(j_fi + j_so + j_si);
+    vd = ((1.0 - p) * (1.0 - v)) / tvm - (p * v) * P.r_tau_vp;
+    wd = ((1.0 - p) * (1.0 - w)) * P.r_tau_wm - (p * w) * P.r_tau_wp;
+}
+
+// The seven non-zero entries of the transposed Jacobian of fk_ion
+// (formula of cu-G:1160-1184): jt[0]=du'/du, jt[1]=dv'/du, jt[2]=dw'/du,
+// jt[3]=du'/dv, jt[4]=dv'/dv, jt[5]=du'/dw, jt[6]=dw'/dw.
+struct JacT {
+    double a0, a1, a2, a3, a4, a5, a6;
+};
+
+__device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, double w) {
+    const double tc = tanh(P.ksm * (u - P.u_c));
+    const double tv = tanh(P.ksm * (u - P.u_v));
+    const double ts = tanh(P.k_fk * (u - P.u_csi));
+    const double p = 0.5 * tc + 0.5;
+    const double q = 0.5 * tv + 0.5;
+    const double dp = 1.0 - tc * tc;
+    const double dq = 1.0 - tv * tv;
+    const double tvm = q * P.tau_v1m + P.tau_v2m * (1.0 - q);
+    const double rtvm = 1.0 / tvm;
+    const double hk = 0.5 * dp * P.ksm;
+    JacT J;
+    J.a0 = -hk * P.r_tau_r + hk * v * (1.0 - u) * (u - P.u_c) * P.r_tau_d + hk * u * P.r_tau_0 +
+           P.k_fk * w * (1.0 - ts * ts) * P.r_2tau_si + p * v * (1.0 - u) * P.r_tau_d -
+           p * v * (u - P.u_c) * P.r_tau_d - (1.0 - p) * P.r_tau_0;
+    J.a3 = p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
+    J.a5 = (ts + 1.0) * P.r_2tau_si;
+    J.a1 = -hk * v * P.r_tau_vp - hk * (1.0 - v) * rtvm +
+           (1.0 - p) * (1.0 - v) * (0.5 * dq * P.ksm * P.dv12) * (rtvm * rtvm);
+    J.a4 = -p * P.r_tau_vp - (1.0 - p) * rtvm;
+    J.a2 = -hk * w * P.r_tau_wp - hk * (1.0 - w) * P.r_tau_wm;
+    J.a6 = -p * P.r_tau_wp - (1.0 - p) * P.r_tau_wm;
+    return J;
+}
+
+// Forward vector field at shared-memory cell q of a region W doubles wide with
+// field planes RN apart: 5-point Laplacian with NaN mirroring + F_ion + E*gh.
+template <int W, int RN>
+__device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restrict__ Y, int q,
+                                       double Egh, double& fu, double& fv, double& fw) {
+    const double u = Y[q];
+    if (isnan(u)) {
+        fu = fv = fw = u;
+        return;
+    }
+    const double v = Y[RN + q], w = Y[2 * RN + q];
+    const double un = Y[q - W], us = Y[q + W], uw = Y[q - 1], ue = Y[q + 1];
+    const bool nN = isnan(un), nS = !nN && isnan(us);
+    const bool nW = isnan(uw), nE = !nW && isnan(ue);
+    const double vn = Y[RN + q - W], vs = Y[RN + q + W], vw = Y[RN + q - 1], ve = Y[RN + q + 1];
+    const double wn = Y[2 * RN + q - W], ws = Y[2 * RN + q + W], ww = Y[2 * RN + q - 1],
+                 we = Y[2 * RN + q + 1];
+    // neighbour pairs after mirroring (cu-F:319-420)
+    const double a_u = nN ? us : un, b_u = nS ? un : us, c_u = nW ? ue : uw, d_u = nE ? uw : ue;
+    const double a_v = nN ? vs : vn, b_v = nS ? vn : vs, c_v = nW ? ve : vw, d_v = nE ? vw : ve;
+    const double a_w = nN ? ws : wn, b_w = nS ? wn : ws, c_w = nW ? we : ww, d_w = nE ? ww : we;
+    const double lu = P.cu * ((((a_u + b_u) + c_u) + d_u) - 4.0 * u);
+    const double lv = P.cv * ((((a_v + b_v) + c_v) + d_v) - 4.0 * v);
+    const double lw = P.cw * ((((a_w + b_w) + c_w) + d_w) - 4.0 * w);
+    double ud, vd, wd;
+    fk_ion(P, u, v, w, ud, vd, wd);
+    fu = (lu + ud) + Egh;
+    fv = lv + vd;
+    fw = lw + wd;
+}
+
+// Weight code of the transposed Laplacian at a cell: 2 bits per direction
+// (north, south, west, east), value 0 (neighbour missing), 1, or 2 (the
+// neighbour mirrored this cell); rule of cu-G:1004-1111.
+__device__ __forceinline__ int wcode_n(int c) { return c & 3; }
+__device__ __forceinline__ int wcode_s(int c) { return (c >> 2) & 3; }
+__device__ __forceinline__ int wcode_w(int c) { return (c >> 4) & 3; }
+__device__ __forceinline__ int wcode_e(int c) { return (c >> 6) & 3; }
+
+// Adjoint vector field L^T z + J_F(y)^T z at shared-memory cell q.
+template <int W, int RN>
+__device__ __forceinline__ void adj_at(const DevModel& P, const double* __restrict__ Z, int q,
+                                       int code, const JacT& J, double& gu, double& gv,
+                                       double& gw) {
+    const double z0 = Z[q], z1 = Z[RN + q], z2 = Z[2 * RN + q];
+    const double pn = (double)wcode_n(code), ps = (double)wcode_s(code);
+    const double pw = (double)wcode_w(code), pe = (double)wcode_e(code);
+    double l[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        const double* Zf = Z + f * RN;
+        const double vn = pn != 0.0 ? Zf[q - W] : 0.0;
+        const double vs = ps != 0.0 ? Zf[q + W] : 0.0;
+        const double vw = pw != 0.0 ? Zf[q - 1] : 0.0;
+        const double ve = pe != 0.0 ? Zf[q + 1] : 0.0;
+        const double c = f == 0 ? P.cu : (f == 1 ? P.cv : P.cw);
+        l[f] = c * ((((pn * vn + ps * vs) + pw * vw) + pe * ve) - 4.0 * Zf[q]);
+    }
+    gu = l[0] + ((J.a0 * z0 + J.a1 * z1) + J.a2 * z2);
+    gv = l[1] + (J.a3 * z0 + J.a4 * z1);
+    gw = l[2] + (J.a5 * z0 + J.a6 * z2);
+}
+
+}  // namespace fkadj

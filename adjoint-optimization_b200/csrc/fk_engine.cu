@@ -1,0 +1,753 @@
+// fk_engine.cu -- host drivers of the FK forward / adjoint engine and the C ABI.
+//
+// Compared with the reference drivers (fk_forward_Et_comp, cu-F:646-849;
+// fk_grad_Et_comp, cu-G:1569-1938) nothing crosses PCIe inside the time loops:
+// the trajectory stays on the device (all states, or sqrt(nt) checkpoints with
+// segment recompute), the objective at T and the z.gh reductions run on the
+// device, and the host only uploads the inputs and downloads gradE once.
+#include "fk_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace fkadj {
+
+static thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+
+#define CK(call, what)                                  \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return fail_cuda(e_, what); \
+    } while (0)
+
+static DevModel make_model(const fkadj_params& p, double dt) {
+    DevModel M;
+    M.u_c = p.u_c;
+    M.u_v = p.u_v;
+    M.ksm = p.ksm;
+    M.k_fk = p.k_fk;
+    M.u_csi = p.u_csi;
+    M.r_tau_d = 1.0 / p.tau_d;
+    M.r_tau_0 = 1.0 / p.tau_0;
+    M.r_tau_r = 1.0 / p.tau_r;
+    M.r_2tau_si = 1.0 / (2 * p.tau_si);
+    M.tau_v1m = p.tau_v1_minus;
+    M.tau_v2m = p.tau_v2_minus;
+    M.r_tau_vp = 1.0 / p.tau_v_plus;
+    M.r_tau_wm = 1.0 / p.tau_w_minus;
+    M.r_tau_wp = 1.0 / p.tau_w_plus;
+    M.dv12 = p.tau_v2_minus - p.tau_v1_minus;
+    M.cu = p.Du / (p.h * p.h);
+    M.cv = p.Dv / (p.h * p.h);
+    M.cw = p.Dw / (p.h * p.h);
+    M.dt = dt;
+    return M;
+}
+
+// Hermite weights (cu-G:1217-1241 and the 27/64 of cu-G:1295-1298).
+static HermiteW make_hermite() {
+    HermiteW w;
+    double t = 1.0 / 3.0;
+    w.c3[0] = (t - 1.0) * (t - 1.0) * (2.0 * t + 1.0);
+    w.c3[1] = t * (t - 1.0) * (t - 1.0);
+    w.c3[2] = t * t * (3.0 - 2.0 * t);
+    w.c3[3] = t * t * (t - 1.0);
+    t = 0.5;
+    w.c4[0] = (1.0 + 2.0 * t + 9.0 * t * t) * (t - 1.0) * (t - 1.0);
+    w.c4[1] = t * (t - 1.0) * (t - 1.0);
+    w.c4[2] = -t * t * (6.0 - 16.0 * t + 9.0 * t * t);
+    w.c4[3] = (t - 1.0) * (9.0 * t - 5.0) * t * t / 4.0;
+    w.c2 = 27.0 * t * t * (t - 1.0) * (t - 1.0) / 4.0;
+    return w;
+}
+
+static inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+static std::mutex g_init_mu;
+static bool g_init_done[64];
+
+Problem::~Problem() {
+    for (auto& r : prof_pool_) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+    if (own_stream_ && st_) cudaStreamDestroy(st_);
+    delete spline_;
+}
+
+fkadj_status Problem::fail_cuda(cudaError_t e, const char* what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? FKADJ_ERR_NOMEM : FKADJ_ERR_CUDA;
+}
+
+fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* ai, int nrows, int ncols,
+                           int n_num, const double* gh_num, const double* gamma, int64_t S_ncol,
+                           const int64_t* S_colptr, const int64_t* S_rowidx, const double* S_val,
+                           double alpha, const fkadj_options* opt, bool need_objective) {
+    fkadj_options o;
+    fkadj_default_options(&o);
+    if (opt) o = *opt;
+    if (!(dt > 0) || nt < 3 || nrows < 2 || ncols < 2 || !ai || !gh_num || n_num < 1) {
+        set_error("invalid argument: need dt > 0, nt >= 3, nrows, ncols >= 2, active_index, gh_num");
+        return FKADJ_ERR_ARG;
+    }
+    if ((int64_t)nrows * ncols > (int64_t)1 << 31) {
+        set_error("grid too large");
+        return FKADJ_ERR_ARG;
+    }
+    const int n = nrows * ncols;
+    int count = 0;
+    for (int k = 0; k < n; ++k) {
+        if (ai[k] < 0 || ai[k] > n_num) {
+            set_error("active_index entry out of range");
+            return FKADJ_ERR_ARG;
+        }
+        count += ai[k] > 0;
+    }
+    if (count != n_num) {
+        set_error("n_num does not match the number of active cells");
+        return FKADJ_ERR_ARG;
+    }
+    if (need_objective) {
+        if (!gamma || !S_colptr || !S_rowidx || !S_val) {
+            set_error("objective needs gamma and S");
+            return FKADJ_ERR_ARG;
+        }
+        if (S_ncol != n_num) {
+            set_error("number of columns of S does not equal the number of active cells");
+            return FKADJ_ERR_ARG;
+        }
+    }
+    p_ = p;
+    dt_ = dt;
+    nt_ = nt;
+    n_num_ = n_num;
+    alpha_ = alpha;
+    if (gamma) std::copy(gamma, gamma + 3, gamma_);
+    grad_mode_ = o.grad_mode;
+    ckpt_policy_ = o.ckpt_policy;
+    if (o.device >= 0) CK(cudaSetDevice(o.device), "cudaSetDevice");
+    CK(cudaGetDevice(&device_), "cudaGetDevice");
+    {
+        std::lock_guard<std::mutex> lk(g_init_mu);
+        if (device_ < 64 && !g_init_done[device_]) {
+            CK(kernels_init(), "kernel attribute setup");
+            g_init_done[device_] = true;
+        }
+    }
+    if (o.stream) {
+        st_ = static_cast<cudaStream_t>(o.stream);
+    } else {
+        CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+        own_stream_ = true;
+    }
+    for (auto& e : ev_) CK(cudaEventCreate(&e), "cudaEventCreate");
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+    ckpt_budget_ = o.ckpt_budget_bytes > 0 ? o.ckpt_budget_bytes : (int64_t)(0.6 * (double)fr);
+
+    g_.nrows = nrows;
+    g_.ncols = ncols;
+    g_.ld = round_up(round_up(ncols, 64) + 2 * HALO, 8);
+    g_.rows_alloc = round_up(nrows, 64) + 2 * HALO;
+    g_.plane = (long long)g_.rows_alloc * g_.ld;
+    P_ = make_model(p, dt);
+    hw_ = make_hermite();
+    tile_ = (o.tile > 0 && o.tile < tile_count()) ? o.tile : 0;
+    ntiles_ = 0;
+    for (int t = 0; t < tile_count(); ++t) ntiles_ = std::max(ntiles_, tiles_of(t, g_));
+
+    // geometry on the padded grid: gh, adjoint stencil weights, compact positions
+    const size_t pl = (size_t)g_.plane;
+    std::vector<double> gh(pl, std::nan(""));
+    std::vector<uint8_t> wc(pl, 0);
+    std::vector<long long> pos(n_num);
+    auto act = [&](int i, int j) { return i >= 0 && i < nrows && j >= 0 && j < ncols && ai[i * ncols + j] > 0; };
+    auto weight = [&](int i, int j, int di, int dj) {
+        if (!act(i + di, j + dj)) return 0;
+        return act(i + 2 * di, j + 2 * dj) ? 1 : 2;
+    };
+    const double ghs = p.Du * 2 / p.h;
+    for (int i = 0; i < nrows; ++i)
+        for (int j = 0; j < ncols; ++j) {
+            const int a = ai[i * ncols + j];
+            if (a <= 0) continue;
+            const size_t o2 = (size_t)(i + HALO) * g_.ld + (j + HALO);
+            gh[o2] = ghs * gh_num[a - 1];
+            wc[o2] = (uint8_t)(weight(i, j, -1, 0) | weight(i, j, 1, 0) << 2 | weight(i, j, 0, -1) << 4 |
+                               weight(i, j, 0, 1) << 6);
+            pos[a - 1] = (long long)o2;
+        }
+    CK(gh_.alloc(pl * sizeof(double)), "alloc gh");
+    CK(wc_.alloc(pl), "alloc weights");
+    CK(pos_.alloc((size_t)n_num * sizeof(long long)), "alloc positions");
+    CK(cudaMemcpy(gh_.p, gh.data(), pl * sizeof(double), cudaMemcpyHostToDevice), "upload gh");
+    CK(cudaMemcpy(wc_.p, wc.data(), pl, cudaMemcpyHostToDevice), "upload weights");
+    CK(cudaMemcpy(pos_.p, pos.data(), (size_t)n_num * sizeof(long long), cudaMemcpyHostToDevice),
+       "upload positions");
+
+    if (need_objective) {
+        // CSC (columns) -> CSR (rows) so that row sums run in ascending column order
+        const int64_t nnz = S_colptr[n_num];
+        std::vector<long long> rp(n_num + 1, 0);
+        for (int64_t k = 0; k < nnz; ++k) {
+            const int64_t r = S_rowidx[k];
+            if (r < 0 || r >= n_num) {
+                set_error("S row index out of range");
+                return FKADJ_ERR_ARG;
+            }
+            rp[r + 1]++;
+        }
+        for (int r = 0; r < n_num; ++r) rp[r + 1] += rp[r];
+        std::vector<int> ci(nnz);
+        std::vector<double> cv(nnz);
+        std::vector<long long> fill(rp.begin(), rp.end() - 1);
+        for (int c = 0; c < n_num; ++c)
+            for (int64_t k = S_colptr[c]; k < S_colptr[c + 1]; ++k) {
+                const long long d = fill[S_rowidx[k]]++;
+                ci[d] = c;
+                cv[d] = S_val[k];
+            }
+        CK(Srow_.alloc((n_num + 1) * sizeof(long long)), "alloc S");
+        CK(Scol_.alloc(std::max<int64_t>(nnz, 1) * sizeof(int)), "alloc S");
+        CK(Sval_.alloc(std::max<int64_t>(nnz, 1) * sizeof(double)), "alloc S");
+        CK(cudaMemcpy(Srow_.p, rp.data(), (n_num + 1) * sizeof(long long), cudaMemcpyHostToDevice), "upload S");
+        if (nnz) {
+            CK(cudaMemcpy(Scol_.p, ci.data(), nnz * sizeof(int), cudaMemcpyHostToDevice), "upload S");
+            CK(cudaMemcpy(Sval_.p, cv.data(), nnz * sizeof(double), cudaMemcpyHostToDevice), "upload S");
+        }
+        have_obj_ = true;
+    }
+    CK(yc_.alloc((size_t)3 * n_num * sizeof(double)), "alloc compact");
+    CK(zc_.alloc((size_t)3 * n_num * sizeof(double)), "alloc compact");
+    CK(opart_.alloc((size_t)objective_blocks(n_num) * sizeof(double)), "alloc partials");
+    CK(osum_.alloc(sizeof(double)), "alloc sum");
+    CK(work_.alloc(3 * state_bytes()), "alloc states");
+    CK(cudaMemset(work_.p, 0xff, work_.bytes), "init states");
+    spline_ = new NakSpline(nt + 1, dt);
+    return FKADJ_OK;
+}
+
+int64_t Problem::device_bytes() const {
+    const DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_,
+                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &y0res_};
+    int64_t s = 0;
+    for (auto* b : all) s += (int64_t)b->bytes;
+    return s;
+}
+
+fkadj_status Problem::prepare_E(const double* Et) {
+    for (int k = 0; k < K_COUNT; ++k) kcount_[k] = ksamples_[k] = 0, kms_[k] = 0.0;
+    prof_used_ = 0;
+    prof_every_ = std::max(1, nt_ / 100);
+    if (!Et) {
+        set_error("Et is null");
+        return FKADJ_ERR_ARG;
+    }
+    Et_.assign(Et, Et + nt_ + 1);
+    ypp_.assign(nt_ + 1, 0.0);
+    spline_->second_derivs(Et_.data(), ypp_.data());
+    Eh_.resize(nt_);
+    E3_.resize(nt_);
+    for (int i = 0; i < nt_; ++i) {
+        Eh_[i] = spline_->value(Et_.data(), ypp_.data(), (i + 0.5) * dt_);          // cu-G:1692-1694
+        E3_[i] = spline_->value(Et_.data(), ypp_.data(), (i + 1.0 / 3.0) * dt_);    // cu-G:1877-1879
+    }
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::upload_state(const double* y_ini, double* d_state) {
+    if (!y0res_.p) {
+        CK(y0res_.alloc(state_bytes()), "alloc initial state");
+        CK(cudaMemsetAsync(y0res_.p, 0xff, y0res_.bytes, st_), "init initial state");
+    }
+    if (y_ini) {
+        CK(cudaMemcpyAsync(yc_.p, y_ini, (size_t)3 * n_num_ * sizeof(double), cudaMemcpyHostToDevice, st_),
+           "upload y_ini");
+        CK(launch_scatter(g_, yc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, y0res_.as<double>(), st_),
+           "scatter");
+        ++launches_;
+        have_y0_ = true;
+    } else if (!have_y0_) {
+        set_error("y_ini is null and no initial state is resident");
+        return FKADJ_ERR_ARG;
+    }
+    CK(cudaMemcpyAsync(d_state, y0res_.p, state_bytes(), cudaMemcpyDeviceToDevice, st_), "copy initial state");
+    return FKADJ_OK;
+}
+
+cudaError_t Problem::prof_begin(int k) {
+    prof_open_ = false;
+    if (!profiling_ || (kcount_[k]++ % prof_every_) != 0) return cudaSuccess;
+    if (prof_used_ == prof_pool_.size()) {
+        ProfRec r{k, nullptr, nullptr};
+        cudaError_t e = cudaEventCreate(&r.a);
+        if (e == cudaSuccess) e = cudaEventCreate(&r.b);
+        if (e != cudaSuccess) return e;
+        prof_pool_.push_back(r);
+    }
+    prof_pool_[prof_used_].k = k;
+    prof_open_ = true;
+    return cudaEventRecord(prof_pool_[prof_used_].a, st_);
+}
+
+cudaError_t Problem::prof_end(int k) {
+    (void)k;
+    if (!prof_open_) return cudaSuccess;
+    prof_open_ = false;
+    return cudaEventRecord(prof_pool_[prof_used_++].b, st_);
+}
+
+fkadj_status Problem::prof_collect() {
+    if (!prof_used_) return FKADJ_OK;
+    CK(cudaStreamSynchronize(st_), "synchronize");
+    for (size_t q = 0; q < prof_used_; ++q) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, prof_pool_[q].a, prof_pool_[q].b), "event time");
+        kms_[prof_pool_[q].k] += ms;
+        ksamples_[prof_pool_[q].k]++;
+    }
+    prof_used_ = 0;
+    return FKADJ_OK;
+}
+
+void Problem::kernel_time(int k, double* avg_ms, int64_t* samples) const {
+    if (k < 0 || k >= K_COUNT) return;
+    if (avg_ms) *avg_ms = ksamples_[k] ? kms_[k] / (double)ksamples_[k] : 0.0;
+    if (samples) *samples = ksamples_[k];
+}
+
+fkadj_status Problem::step_forward(int i, const double* yin, double* yout) {
+    CK(prof_begin(K_FWD), "profiling event");
+    CK(launch_fwd_step(tile_, P_, g_, yin, yout, gh_.as<double>(), Et_[i], Eh_[i], Et_[i + 1], st_),
+       "forward step");
+    CK(prof_end(K_FWD), "profiling event");
+    ++launches_;
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::download_grid(const double* d_state, double* host) {
+    const size_t n = (size_t)g_.nrows * g_.ncols;
+    for (int f = 0; f < 3; ++f) {
+        const double* src = d_state + (size_t)f * g_.plane + (size_t)HALO * g_.ld + HALO;
+        CK(cudaMemcpy2DAsync(host + f * n, g_.ncols * sizeof(double), src, g_.ld * sizeof(double),
+                             g_.ncols * sizeof(double), g_.nrows, cudaMemcpyDeviceToHost, st_),
+           "download state");
+    }
+    CK(cudaStreamSynchronize(st_), "synchronize");
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::forward(const double* Et, const double* y_ini, int nstep, int ns, double* ys, double* yf) {
+    fkadj_status s;
+    launches_ = 0;
+    if ((s = prepare_E(Et))) return s;
+    if (ns > 0 && (!ys || nstep <= 0)) {
+        set_error("ys and nstep > 0 are needed when ns > 0");
+        return FKADJ_ERR_ARG;
+    }
+    CK(cudaEventRecord(ev_[0], st_), "event");
+    double* b0 = state_buf(0);
+    if ((s = upload_state(y_ini, b0))) return s;
+    double* cur = b0;
+    const size_t n3 = (size_t)3 * g_.nrows * g_.ncols;
+    for (int i = 0; i < nt_; ++i) {
+        double* out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
+        if ((s = step_forward(i, cur, out))) return s;
+        cur = out;
+        if (nstep > 0 && (i + 1) % nstep == 0) {  // snapshots (cu-F:794-814)
+            const int ks = (i + 1) / nstep - 1;
+            if (ks < ns && (s = download_grid(cur, ys + (size_t)ks * n3))) return s;
+        }
+    }
+    CK(cudaEventRecord(ev_[1], st_), "event");
+    CK(cudaEventRecord(ev_[2], st_), "event");
+    if (yf) {
+        if ((s = download_grid(cur, yf))) return s;
+    }
+    CK(cudaStreamSynchronize(st_), "synchronize");
+    if ((s = prof_collect())) return s;
+    float a = 0;
+    cudaEventElapsedTime(&a, ev_[0], ev_[1]);
+    timing_.fwd_ms = a;
+    timing_.bwd_ms = 0;
+    timing_.total_ms = a;
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::run_objective(const double* yT, double* L0) {
+    if (!have_obj_) {
+        set_error("problem has no objective");
+        return FKADJ_ERR_ARG;
+    }
+    CK(launch_gather(g_, yT, n_num_, pos_.as<long long>(), yc_.as<double>(), st_), "gather");
+    CK(launch_objective(yc_.as<double>(), n_num_, Srow_.as<long long>(), Scol_.as<int>(), Sval_.as<double>(),
+                        gamma_, zc_.as<double>(), opart_.as<double>(), st_),
+       "objective");
+    CK(launch_sum_rows(opart_.as<double>(), 1, objective_blocks(n_num_), osum_.as<double>(), st_), "sum");
+    launches_ += 3;
+    double s = 0;
+    CK(cudaMemcpyAsync(&s, osum_.p, sizeof(double), cudaMemcpyDeviceToHost, st_), "download L0");
+    CK(cudaStreamSynchronize(st_), "synchronize");
+    *L0 = -s;
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::objective(const double* Et, const double* y_ini, double* L0, double* LE, double* Lcost,
+                                double* yf) {
+    fkadj_status s;
+    launches_ = 0;
+    if ((s = prepare_E(Et))) return s;
+    CK(cudaEventRecord(ev_[0], st_), "event");
+    double* cur = state_buf(0);
+    if ((s = upload_state(y_ini, cur))) return s;
+    for (int i = 0; i < nt_; ++i) {
+        double* out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
+        if ((s = step_forward(i, cur, out))) return s;
+        cur = out;
+    }
+    CK(cudaEventRecord(ev_[1], st_), "event");
+    double l0 = 0;
+    if ((s = run_objective(cur, &l0))) return s;
+    CK(cudaEventRecord(ev_[2], st_), "event");
+    double le = 0;
+    for (int i = 0; i <= nt_; ++i) le += Et_[i] * Et_[i];
+    le *= dt_;
+    if (L0) *L0 = l0;
+    if (LE) *LE = le;
+    if (Lcost) *Lcost = 0.5 * l0 + 0.5 * alpha_ * le;
+    if (yf && (s = download_grid(cur, yf))) return s;
+    CK(cudaStreamSynchronize(st_), "synchronize");
+    if ((s = prof_collect())) return s;
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ev_[0], ev_[1]);
+    cudaEventElapsedTime(&b, ev_[0], ev_[2]);
+    timing_.fwd_ms = a;
+    timing_.bwd_ms = 0;
+    timing_.total_ms = b;
+    if (!std::isfinite(l0)) {
+        set_error("objective is not finite");
+        return FKADJ_ERR_NUMERIC;
+    }
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::plan_trajectory(TrajPlan& tp) {
+    const double sb = (double)state_bytes();
+    int pol = ckpt_policy_;
+    if (pol == FKADJ_CKPT_AUTO) pol = ((double)(nt_ + 1) * sb <= (double)ckpt_budget_) ? FKADJ_CKPT_FULL : FKADJ_CKPT_SQRT;
+    if (pol == FKADJ_CKPT_BINOMIAL) pol = FKADJ_CKPT_SQRT;
+    tp.policy = pol;
+    if (pol == FKADJ_CKPT_FULL) {
+        tp.stride = 1;
+        tp.nslots = nt_ + 1;
+        tp.seg_slots = 0;
+    } else {
+        const int c = std::max(2, (int)std::ceil(std::sqrt((double)nt_)));
+        tp.stride = c;
+        tp.nslots = (nt_ + c - 1) / c + 1;
+        tp.seg_slots = c - 1;
+    }
+    const double need = (double)(tp.nslots + tp.seg_slots) * sb;
+    if (ckpt_policy_ != FKADJ_CKPT_FULL && need > (double)ckpt_budget_) {
+        set_error("trajectory store does not fit the checkpoint budget");
+        return FKADJ_ERR_NOMEM;
+    }
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
+    if (traj_.p && traj_plan_.policy == tp.policy && traj_plan_.nslots == tp.nslots &&
+        traj_plan_.seg_slots == tp.seg_slots)
+        return FKADJ_OK;
+    traj_.release();
+    seg_.release();
+    CK(traj_.alloc((size_t)tp.nslots * state_bytes()), "alloc trajectory");
+    CK(cudaMemsetAsync(traj_.p, 0xff, traj_.bytes, st_), "init trajectory");
+    if (tp.seg_slots) {
+        CK(seg_.alloc((size_t)tp.seg_slots * state_bytes()), "alloc segment buffer");
+        CK(cudaMemsetAsync(seg_.p, 0xff, seg_.bytes, st_), "init segment buffer");
+    }
+    traj_plan_ = tp;
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, double* LE, double* Lcost,
+                           double* gradE, double* yf) {
+    fkadj_status s;
+    launches_ = 0;
+    if (!gradE) {
+        set_error("gradE is null");
+        return FKADJ_ERR_ARG;
+    }
+    if (grad_mode_ != FKADJ_GRAD_REF) {
+        set_error("gradient mode not available");
+        return FKADJ_ERR_ARG;
+    }
+    if ((s = prepare_E(Et))) return s;
+    TrajPlan tp;
+    if ((s = plan_trajectory(tp))) return s;
+    if ((s = ensure_traj(tp))) return s;
+    if (!zbuf_.p) {
+        CK(zbuf_.alloc(2 * state_bytes()), "alloc adjoint states");
+        CK(cudaMemsetAsync(zbuf_.p, 0xff, zbuf_.bytes, st_), "init adjoint states");
+        CK(yh_.alloc(state_bytes()), "alloc midpoint state");
+        CK(cudaMemsetAsync(yh_.p, 0xff, yh_.bytes, st_), "init midpoint state");
+    }
+    const size_t pbytes = (size_t)(nt_ + 1) * ntiles_ * sizeof(double);
+    if (partial_.bytes < pbytes) {
+        CK(partial_.alloc(pbytes), "alloc partials");
+        CK(zgh_.alloc((size_t)(nt_ + 1) * sizeof(double)), "alloc zgh");
+    }
+    const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
+    const int ntl = tiles_of(tile_, g_);
+    CK(cudaEventRecord(ev_[0], st_), "event");
+    // ---- forward sweep, storing states (cu-G:1689-1724 without the D2H copies)
+    if ((s = upload_state(y_ini, slot(0)))) return s;
+    double* cur = slot(0);
+    for (int i = 0; i < nt; ++i) {
+        double* out;
+        if (tp.policy == FKADJ_CKPT_FULL) out = slot(i + 1);
+        else if ((i + 1) % c == 0) out = slot((i + 1) / c);
+        else if (i + 1 == nt) out = slot(K);
+        else out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
+        if ((s = step_forward(i, cur, out))) return s;
+        cur = out;
+    }
+    double* yT = cur;
+    CK(cudaEventRecord(ev_[1], st_), "event");
+    // ---- objective and terminal adjoint state z(T) = -gamma S y(T) (cu-G:1769-1838)
+    double l0 = 0;
+    if ((s = run_objective(yT, &l0))) return s;
+    double* z = zbuf_.as<double>();
+    double* z2 = z + state_elems();
+    CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, z, st_), "scatter z");
+    double* part = partial_.as<double>();
+    CK(launch_dot_gh(tile_, g_, z, gh_.as<double>(), part + (size_t)nt * ntl, st_), "z.gh");
+    launches_ += 2;
+    // ---- backward sweep (cu-G:1866-1908)
+    auto back_step = [&](int i, const double* ya, const double* yb) -> fkadj_status {
+        CK(prof_begin(K_MID), "profiling event");
+        CK(launch_adj_mid(tile_, P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), Et_[i - 1], Et_[i],
+                          E3_[i - 1], hw_, st_),
+           "adjoint midpoint");
+        CK(prof_end(K_MID), "profiling event");
+        CK(prof_begin(K_ADJ), "profiling event");
+        CK(launch_adj_step(tile_, P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(), gh_.as<double>(),
+                           part + (size_t)(i - 1) * ntl, st_),
+           "adjoint step");
+        CK(prof_end(K_ADJ), "profiling event");
+        launches_ += 2;
+        std::swap(z, z2);
+        return FKADJ_OK;
+    };
+    if (tp.policy == FKADJ_CKPT_FULL) {
+        for (int i = nt; i > 0; --i)
+            if ((s = back_step(i, slot(i - 1), slot(i)))) return s;
+    } else {
+        for (int k = K - 1; k >= 0; --k) {
+            const int s0 = k * c, s1 = std::min(s0 + c, nt);
+            auto st = [&](int t) -> double* {
+                if (t == s0) return slot(k);
+                if (t == s1) return slot(k + 1);
+                return segslot(t - s0 - 1);
+            };
+            for (int t = s0; t < s1 - 1; ++t)
+                if ((s = step_forward(t, st(t), st(t + 1)))) return s;
+            for (int i = s1; i > s0; --i)
+                if ((s = back_step(i, st(i - 1), st(i)))) return s;
+        }
+    }
+    CK(launch_sum_rows(part, nt + 1, ntl, zgh_.as<double>(), st_), "reduce z.gh");
+    ++launches_;
+    std::vector<double> zgh(nt + 1);
+    CK(cudaMemcpyAsync(zgh.data(), zgh_.p, (nt + 1) * sizeof(double), cudaMemcpyDeviceToHost, st_),
+       "download z.gh");
+    CK(cudaEventRecord(ev_[2], st_), "event");
+    if (yf && (s = download_grid(yT, yf))) return s;
+    CK(cudaStreamSynchronize(st_), "synchronize");
+    if ((s = prof_collect())) return s;
+    double le = 0;
+    for (int i = 0; i <= nt; ++i) le += Et_[i] * Et_[i];
+    le *= dt_;
+    for (int i = 0; i <= nt; ++i) gradE[i] = alpha_ * Et_[i] - zgh[i];  // cu-G:1924-1926
+    if (L0) *L0 = l0;
+    if (LE) *LE = le;
+    if (Lcost) *Lcost = 0.5 * l0 + 0.5 * alpha_ * le;
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ev_[0], ev_[1]);
+    cudaEventElapsedTime(&b, ev_[0], ev_[2]);
+    timing_.fwd_ms = a;
+    timing_.bwd_ms = b - a;
+    timing_.total_ms = b;
+    if (!std::isfinite(l0)) {
+        set_error("objective is not finite");
+        return FKADJ_ERR_NUMERIC;
+    }
+    return FKADJ_OK;
+}
+
+}  // namespace fkadj
+
+// ======================================================================= C ABI
+using fkadj::Problem;
+
+struct fkadj_problem {
+    Problem impl;
+};
+
+extern "C" {
+
+void fkadj_default_options(fkadj_options* opt) {
+    if (!opt) return;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->grad_mode = FKADJ_GRAD_REF;
+    opt->ckpt_policy = FKADJ_CKPT_AUTO;
+    opt->ckpt_budget_bytes = 0;
+    opt->device = -1;
+    opt->stream = nullptr;
+    opt->tile = 0;
+    opt->verbose = 0;
+}
+
+void fkadj_default_params(fkadj_params* p, double dx) {
+    if (!p) return;
+    // src/cuda/fk_parameters_00_05_alpha_0p8_dx_0p035.h:2-23 (h := dx)
+    p->u_c = 0.13;
+    p->u_v = 0.04;
+    p->tau_d = 0.388;
+    p->tau_v1_minus = 7.6;
+    p->tau_v2_minus = 8.8;
+    p->tau_v_plus = 3.324;
+    p->tau_0 = 8.2;
+    p->tau_r = 33.264;
+    p->tau_si = 29.0;
+    p->u_csi = 0.54;
+    p->k_fk = 15.0;
+    p->tau_w_minus = 68.0;
+    p->tau_w_plus = 399.99999999999994;
+    p->Du = 1.0e-3;
+    p->Dv = 1.0e-5;
+    p->Dw = 1.0e-5;
+    p->ksm = 100.0;
+    p->h = dx;
+}
+
+const char* fkadj_last_error(void) { return fkadj::g_err.c_str(); }
+
+const char* fkadj_param_string(const fkadj_params* p) {
+    static thread_local std::string s;
+    if (!p) return "";
+    char buf[2048];
+    std::snprintf(buf, sizeof(buf),
+                  "// Fenton-Karma parameters (runtime)\n"
+                  "u_c = %.17g\nu_v = %.17g\ntau_d = %.17g\ntau_v1_minus = %.17g\ntau_v2_minus = %.17g\n"
+                  "tau_v_plus = %.17g\ntau_0 = %.17g\ntau_r = %.17g\ntau_si = %.17g\nu_csi = %.17g\n"
+                  "k_fk = %.17g\ntau_w_minus = %.17g\ntau_w_plus = %.17g\n\nDu = %.17g\nDv = %.17g\n"
+                  "Dw = %.17g\n\nksm = %.17g\n\nh = %.17g\nnvar = 3\n",
+                  p->u_c, p->u_v, p->tau_d, p->tau_v1_minus, p->tau_v2_minus, p->tau_v_plus, p->tau_0,
+                  p->tau_r, p->tau_si, p->u_csi, p->k_fk, p->tau_w_minus, p->tau_w_plus, p->Du, p->Dv, p->Dw,
+                  p->ksm, p->h);
+    s = buf;
+    return s.c_str();
+}
+
+fkadj_status fkadj_forward(const fkadj_params* p, double dt, const double* Et, int nt, const double* y_ini,
+                           const int* active_index, int nrows, int ncols, int n_num, const double* gh_num,
+                           int nstep, int ns, double* ys, double* yf, const fkadj_options* opt) {
+    if (!p) {
+        fkadj::set_error("params is null");
+        return FKADJ_ERR_ARG;
+    }
+    Problem pb;
+    fkadj_status s = pb.init(*p, dt, nt, active_index, nrows, ncols, n_num, gh_num, nullptr, 0, nullptr, nullptr,
+                             nullptr, 0.0, opt, false);
+    if (s) return s;
+    return pb.forward(Et, y_ini, nstep, ns, ys, yf);
+}
+
+fkadj_status fkadj_grad(const fkadj_params* p, double dt, const double* Et, int nt, const double* y_ini,
+                        const int* active_index, int nrows, int ncols, int n_num, const double* gh_num,
+                        const double* gamma, int64_t S_ncol, const int64_t* S_colptr, const int64_t* S_rowidx,
+                        const double* S_val, double alpha, double* L0, double* LE, double* Lcost, double* gradE,
+                        double* yf, const fkadj_options* opt) {
+    if (!p) {
+        fkadj::set_error("params is null");
+        return FKADJ_ERR_ARG;
+    }
+    Problem pb;
+    fkadj_status s = pb.init(*p, dt, nt, active_index, nrows, ncols, n_num, gh_num, gamma, S_ncol, S_colptr,
+                             S_rowidx, S_val, alpha, opt, true);
+    if (s) return s;
+    return pb.grad(Et, y_ini, L0, LE, Lcost, gradE, yf);
+}
+
+fkadj_status fkadj_problem_create(fkadj_problem** out, const fkadj_params* p, double dt, int nt,
+                                  const int* active_index, int nrows, int ncols, int n_num, const double* gh_num,
+                                  const double* gamma, int64_t S_ncol, const int64_t* S_colptr,
+                                  const int64_t* S_rowidx, const double* S_val, double alpha,
+                                  const fkadj_options* opt) {
+    if (!out || !p) {
+        fkadj::set_error("null argument");
+        return FKADJ_ERR_ARG;
+    }
+    *out = nullptr;
+    auto* h = new (std::nothrow) fkadj_problem;
+    if (!h) return FKADJ_ERR_NOMEM;
+    const bool need_obj = gamma && S_colptr;
+    fkadj_status s = h->impl.init(*p, dt, nt, active_index, nrows, ncols, n_num, gh_num, gamma, S_ncol, S_colptr,
+                                  S_rowidx, S_val, alpha, opt, need_obj);
+    if (s) {
+        delete h;
+        return s;
+    }
+    *out = h;
+    return FKADJ_OK;
+}
+
+void fkadj_problem_destroy(fkadj_problem* pb) { delete pb; }
+
+int64_t fkadj_problem_device_bytes(const fkadj_problem* pb) { return pb ? pb->impl.device_bytes() : 0; }
+
+fkadj_status fkadj_problem_objective(fkadj_problem* pb, const double* Et, const double* y_ini, double* L0,
+                                     double* LE, double* Lcost, double* yf) {
+    if (!pb) return FKADJ_ERR_ARG;
+    return pb->impl.objective(Et, y_ini, L0, LE, Lcost, yf);
+}
+
+fkadj_status fkadj_problem_grad(fkadj_problem* pb, const double* Et, const double* y_ini, double* L0, double* LE,
+                                double* Lcost, double* gradE, double* yf) {
+    if (!pb) return FKADJ_ERR_ARG;
+    return pb->impl.grad(Et, y_ini, L0, LE, Lcost, gradE, yf);
+}
+
+void fkadj_problem_last_timing(const fkadj_problem* pb, double out[3]) {
+    if (!pb || !out) return;
+    const fkadj::Timing t = pb->impl.last_timing();
+    out[0] = t.fwd_ms;
+    out[1] = t.bwd_ms;
+    out[2] = t.total_ms;
+}
+
+int64_t fkadj_problem_last_launches(const fkadj_problem* pb) { return pb ? pb->impl.last_launches() : 0; }
+
+void fkadj_problem_set_profiling(fkadj_problem* pb, int enable) {
+    if (pb) pb->impl.set_profiling(enable != 0);
+}
+
+void fkadj_problem_kernel_time(const fkadj_problem* pb, int kernel, double* avg_ms, int64_t* samples) {
+    if (avg_ms) *avg_ms = 0.0;
+    if (samples) *samples = 0;
+    if (pb) pb->impl.kernel_time(kernel, avg_ms, samples);
+}
+
+}  // extern "C"

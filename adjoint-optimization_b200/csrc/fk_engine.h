@@ -1,0 +1,155 @@
+// fk_engine.h -- resident FK problem: geometry, objective, work buffers and
+// the trajectory store of one instance on one GPU, plus the forward and
+// gradient drivers (the roles of fk_forward_Et_comp, cu-F:646-849, and
+// fk_grad_Et_comp, cu-G:1569-1938).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/fkadj.h"
+#include "fk_kernels.h"
+#include "fk_spline.h"
+
+namespace fkadj {
+
+void set_error(const std::string& msg);
+
+// One device allocation released on destruction.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t b) {
+        release();
+        if (b == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) bytes = b;
+        else p = nullptr;
+        return e;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct Timing {
+    double fwd_ms = 0, bwd_ms = 0, total_ms = 0;
+};
+
+// Where the states y(t_i) live during one gradient.
+struct TrajPlan {
+    int policy = FKADJ_CKPT_FULL;  // resolved policy (FULL / SQRT / BINOMIAL)
+    int stride = 1;                // steps between stored states (SQRT)
+    int nslots = 0;                // stored state slots
+    int seg_slots = 0;             // recompute buffer slots
+};
+
+class Problem {
+public:
+    ~Problem();
+    fkadj_status init(const fkadj_params& p, double dt, int nt, const int* active_index, int nrows,
+                      int ncols, int n_num, const double* gh_num, const double* gamma, int64_t S_ncol,
+                      const int64_t* S_colptr, const int64_t* S_rowidx, const double* S_val, double alpha,
+                      const fkadj_options* opt, bool need_objective);
+
+    fkadj_status forward(const double* Et, const double* y_ini, int nstep, int ns, double* ys, double* yf);
+    fkadj_status objective(const double* Et, const double* y_ini, double* L0, double* LE, double* Lcost,
+                           double* yf);
+    fkadj_status grad(const double* Et, const double* y_ini, double* L0, double* LE, double* Lcost,
+                      double* gradE, double* yf);
+
+    int64_t device_bytes() const;
+    Timing last_timing() const { return timing_; }
+    int64_t last_launches() const { return launches_; }
+
+    // Sampled per-kernel device times (CUDA events around every k-th launch
+    // of each kernel kind; off by default).
+    enum Kernel { K_FWD = 0, K_MID = 1, K_ADJ = 2, K_COUNT = 3 };
+    void set_profiling(bool on) { profiling_ = on; }
+    void kernel_time(int k, double* avg_ms, int64_t* samples) const;
+    const DevGrid& grid() const { return g_; }
+    int nt() const { return nt_; }
+    int n_num() const { return n_num_; }
+    cudaStream_t stream() const { return st_; }
+    int tile() const { return tile_; }
+    void set_tile(int t) { tile_ = t; }
+
+    // Lower-level pieces (used by the batch / serving layers and the tests).
+    // upload_state with y_ini == nullptr re-uses the initial state of the
+    // previous call (kept resident on the device).
+    fkadj_status upload_state(const double* y_ini, double* d_state);
+    fkadj_status prepare_E(const double* Et);
+    fkadj_status step_forward(int i, const double* yin, double* yout);
+    double* state_buf(int k) const { return work_.as<double>() + (size_t)k * state_elems(); }
+    size_t state_elems() const { return (size_t)3 * g_.plane; }
+    size_t state_bytes() const { return state_elems() * sizeof(double); }
+
+private:
+    fkadj_status fail_cuda(cudaError_t e, const char* what);
+    // brackets a launch of kernel kind k with sampled events when profiling
+    cudaError_t prof_begin(int k);
+    cudaError_t prof_end(int k);
+    fkadj_status prof_collect();
+    fkadj_status plan_trajectory(TrajPlan& tp);
+    fkadj_status ensure_traj(const TrajPlan& tp);
+    fkadj_status run_objective(const double* yT, double* L0);
+    fkadj_status download_grid(const double* d_state, double* host_dense);
+    double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
+    double* segslot(int k) const { return seg_.as<double>() + (size_t)k * state_elems(); }
+
+    fkadj_params p_{};
+    DevModel P_{};
+    DevGrid g_{};
+    HermiteW hw_{};
+    double dt_ = 0, alpha_ = 0, gamma_[3] = {0, 0, 0};
+    int nt_ = 0, n_num_ = 0, tile_ = 0, device_ = 0, ntiles_ = 0;
+    bool own_stream_ = false, have_obj_ = false;
+    int grad_mode_ = FKADJ_GRAD_REF, ckpt_policy_ = FKADJ_CKPT_AUTO;
+    int64_t ckpt_budget_ = 0;
+    cudaStream_t st_ = nullptr;
+    cudaEvent_t ev_[3] = {nullptr, nullptr, nullptr};
+
+    // device buffers
+    DevBuf gh_, wc_, pos_, Srow_, Scol_, Sval_, yc_, zc_, opart_, osum_;
+    DevBuf work_;      // 4 states: two ping-pong, z pair is separate
+    DevBuf zbuf_;      // 2 adjoint states
+    DevBuf yh_;        // midpoint state
+    DevBuf partial_;   // (nt+1) x ntiles zgh partials
+    DevBuf zgh_;       // nt+1
+    DevBuf traj_, seg_;
+    DevBuf y0res_;     // resident initial state
+    bool have_y0_ = false;
+    TrajPlan traj_plan_{};
+
+    // sampled kernel timing
+    bool profiling_ = false;
+    int prof_every_ = 1;
+    int64_t kcount_[K_COUNT] = {0, 0, 0};
+    int64_t ksamples_[K_COUNT] = {0, 0, 0};
+    double kms_[K_COUNT] = {0, 0, 0};
+    struct ProfRec {
+        int k;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfRec> prof_pool_;
+    size_t prof_used_ = 0;
+    bool prof_open_ = false;
+
+    // host
+    std::vector<double> Et_, ypp_, Eh_, E3_;
+    NakSpline* spline_ = nullptr;
+    Timing timing_{};
+    int64_t launches_ = 0;
+};
+
+}  // namespace fkadj

@@ -1,0 +1,529 @@
+// fk_kernels.cu -- sm_100a kernels of the FK forward / adjoint engine.
+//
+// Every time step is one fused launch.  A CTA owns a TX x TY tile of the grid,
+// stages the tile plus a HALO-wide ring of each field into shared memory once,
+// and runs all four RK stages out of shared memory: stage s is evaluated on the
+// tile grown by (4 - s) cells, so the halo shrinks by one cell per stage and no
+// stage needs another CTA's data (temporal blocking over the RK stages).
+// Global traffic per cell and step is therefore one read and one write of the
+// state plus gh (56 B), instead of the reference's four launches and ~440 B
+// (cu-F:766-793).  The work is FP64 arithmetic (3 tanh per vector-field
+// evaluation), so the tile shape trades halo recompute against occupancy.
+#include "fk_kernels.h"
+
+#include <cstdio>
+
+namespace fkadj {
+
+namespace {
+
+// Copies a rows x width window of the three planes at src (row pitch ld, plane
+// pitch plane) into shared memory (row pitch width, plane pitch rn), with
+// 16-byte vector loads when the window is 16-byte aligned.
+template <int ROWS, int WIDTH, int NT>
+__device__ __forceinline__ void load_region(double* __restrict__ dst, const double* __restrict__ src,
+                                            int ld, long long plane, bool vec_ok) {
+    constexpr int RN = ROWS * WIDTH;
+    if (vec_ok && (WIDTH % 2) == 0) {
+        constexpr int HW = WIDTH / 2;
+        for (int q = threadIdx.x; q < 3 * ROWS * HW; q += NT) {
+            const int f = q / (ROWS * HW);
+            const int rem = q - f * (ROWS * HW);
+            const int r = rem / HW, c2 = rem - r * HW;
+            const double2 v = __ldg(reinterpret_cast<const double2*>(src + f * plane + (long long)r * ld) + c2);
+            reinterpret_cast<double2*>(dst + f * RN + r * WIDTH)[c2] = v;
+        }
+    } else {
+        for (int q = threadIdx.x; q < 3 * RN; q += NT) {
+            const int f = q / RN;
+            const int rem = q - f * RN;
+            const int r = rem / WIDTH, c = rem - r * WIDTH;
+            dst[q] = __ldg(src + f * plane + (long long)r * ld + c);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- forward
+
+// One forward RK stage evaluated on the tile grown by E cells.
+//   MODE 0: first stage   Y <- Y0 + cY*k, D  = cD*k
+//   MODE 1: middle stage  Y <- Y0 + cY*k, D += cD*k
+//   MODE 2: last stage    out <- (Y0 + D) + cD*k   (interior only)
+// Stage algebra and E sources of cu-F:459-562 / cu-F:766-793.
+template <int E, int TX, int TY, int NT, int MODE>
+__device__ __forceinline__ void fwd_stage(const DevModel& P, double* __restrict__ Y,
+                                          const double* __restrict__ Y0, double* __restrict__ D,
+                                          const double* __restrict__ ghs, int ld, double Ev,
+                                          double cY, double cD, double* __restrict__ out,
+                                          long long plane) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
+    constexpr int IT = (N + NT - 1) / NT;
+    constexpr int IN = TX * TY;
+    double ku[IT], kv[IT], kw[IT];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = threadIdx.x + it * NT;
+        if (q < N) {
+            const int r = HALO - E + q / W, c = HALO - E + q % W;
+            const double g = __ldg(ghs + (long long)r * ld + c);
+            rhs_at<RW, RN>(P, Y, r * RW + c, Ev * g, ku[it], kv[it], kw[it]);
+        }
+    }
+    if (MODE != 2) __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = threadIdx.x + it * NT;
+        if (q < N) {
+            const int r = HALO - E + q / W, c = HALO - E + q % W;
+            const int s = r * RW + c;
+            const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+            const int d = (r - HALO) * TX + (c - HALO);
+            if (MODE == 2) {
+                const long long o = (long long)r * ld + c;
+                out[o] = (Y0[s] + D[d]) + cD * ku[it];
+                out[plane + o] = (Y0[RN + s] + D[IN + d]) + cD * kv[it];
+                out[2 * plane + o] = (Y0[2 * RN + s] + D[2 * IN + d]) + cD * kw[it];
+            } else {
+                Y[s] = Y0[s] + cY * ku[it];
+                Y[RN + s] = Y0[RN + s] + cY * kv[it];
+                Y[2 * RN + s] = Y0[2 * RN + s] + cY * kw[it];
+                if (inner) {
+                    if (MODE == 0) {
+                        D[d] = cD * ku[it];
+                        D[IN + d] = cD * kv[it];
+                        D[2 * IN + d] = cD * kw[it];
+                    } else {
+                        D[d] = D[d] + cD * ku[it];
+                        D[IN + d] = D[IN + d] + cD * kv[it];
+                        D[2 * IN + d] = D[2 * IN + d] + cD * kw[it];
+                    }
+                }
+            }
+        }
+    }
+    if (MODE != 2) __syncthreads();
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin,
+                                                 double* __restrict__ yout, const double* __restrict__ gh,
+                                                 double E0, double Eh, double E1) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    extern __shared__ double4 smem_raw[];
+    double* Y = reinterpret_cast<double*>(smem_raw);
+    double* Y0 = Y + 3 * RN;
+    double* D = Y0 + 3 * RN;
+    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    // region origin: logical (i0 - HALO, j0 - HALO) = padded (i0, j0)
+    const long long off = (long long)i0 * g.ld + j0;
+    const bool vec_ok = ((g.ld | j0) & 1) == 0;
+    load_region<RH, RW, NT>(Y, yin + off, g.ld, g.plane, vec_ok);
+    __syncthreads();
+    for (int q = threadIdx.x; q < 3 * RN; q += NT) Y0[q] = Y[q];
+    __syncthreads();
+    const double* ghs = gh + off;
+    const double dt = P.dt;
+    fwd_stage<3, TX, TY, NT, 0>(P, Y, Y0, D, ghs, g.ld, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, 0);
+    fwd_stage<2, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, 0);
+    fwd_stage<1, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, 0);
+    fwd_stage<0, TX, TY, NT, 2>(P, Y, Y0, D, ghs, g.ld, E1, 0.0, dt * 1.0 / 6.0, yout + off, g.plane);
+}
+
+// ------------------------------------------------- reference-mode adjoint
+
+// Midpoint state of step [t_{i-1}, t_i] (cu-G:1244-1301): y3 = cubic Hermite
+// at 1/3 from (ya, yb, dt*f(ya), dt*f(yb)); yh = partial quartic at 1/2 plus
+// (27/64) dt f(y3, E(t_{i-1}+dt/3)).  Halo 2: f(ya), f(yb) on the tile grown by
+// one cell, f(y3) on the tile.
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya,
+                                                const double* __restrict__ yb,
+                                                const double* __restrict__ gh, double* __restrict__ yh,
+                                                double Ea, double Eb, double E3, HermiteW hw) {
+    constexpr int H2 = 2;
+    constexpr int RW = TX + 2 * H2, RH = TY + 2 * H2, RN = RW * RH;
+    extern __shared__ double4 smem_raw[];
+    double* A = reinterpret_cast<double*>(smem_raw);
+    double* B = A + 3 * RN;
+    double* C = B + 3 * RN;
+    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    // region origin: logical (i0 - 2, j0 - 2) = padded (i0 + 2, j0 + 2)
+    const long long off = (long long)(i0 + HALO - H2) * g.ld + (j0 + HALO - H2);
+    const bool vec_ok = ((g.ld | (j0 + HALO - H2)) & 1) == 0;
+    load_region<RH, RW, NT>(A, ya + off, g.ld, g.plane, vec_ok);
+    load_region<RH, RW, NT>(B, yb + off, g.ld, g.plane, vec_ok);
+    __syncthreads();
+    const double dt = P.dt;
+    {
+        constexpr int W = TX + 2, N = W * (TY + 2), IT = (N + NT - 1) / NT;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int q = threadIdx.x + it * NT;
+            if (q < N) {
+                const int r = 1 + q / W, c = 1 + q % W;
+                const int s = r * RW + c;
+                const double gg = __ldg(gh + off + (long long)r * g.ld + c);
+                double a0[3], a1[3];
+                rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2]);
+                rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2]);
+                const bool inner = r >= H2 && r < H2 + TY && c >= H2 && c < H2 + TX;
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                    const double m0 = a0[f] * dt, m1 = a1[f] * dt;
+                    const double x0 = A[f * RN + s], x1 = B[f * RN + s];
+                    C[f * RN + s] = ((hw.c3[0] * x0 + hw.c3[1] * m0) + hw.c3[2] * x1) + hw.c3[3] * m1;
+                    if (inner)
+                        yh[off + f * g.plane + (long long)r * g.ld + c] =
+                            ((hw.c4[0] * x0 + hw.c4[1] * m0) + hw.c4[2] * x1) + hw.c4[3] * m1;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // y3 outside the grown tile is never read: stencils of tile cells reach one
+    // cell out.  Cells of C on the outer ring stay unset and unused.
+    {
+        constexpr int N = TX * TY, IT = (N + NT - 1) / NT;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int q = threadIdx.x + it * NT;
+            if (q < N) {
+                const int r = H2 + q / TX, c = H2 + q % TX;
+                const int s = r * RW + c;
+                const double gg = __ldg(gh + off + (long long)r * g.ld + c);
+                double m2[3];
+                rhs_at<RW, RN>(P, C, s, E3 * gg, m2[0], m2[1], m2[2]);
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                    double* p = yh + off + f * g.plane + (long long)r * g.ld + c;
+                    *p = *p + hw.c2 * (m2[f] * dt);
+                }
+            }
+        }
+    }
+}
+
+// Fixed-order block sum (warp shuffles, then warps in order); result valid in
+// thread 0.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int w = 0; w < NT / 32; ++w) s += red[w];
+    }
+    return s;
+}
+
+// One backward RK4 step of the reference adjoint (cu-G:1349-1427 in the order
+// of cu-G:1885-1891): stage 1 uses y(t_i) = yb, stages 2-3 the midpoint yh,
+// stage 4 y(t_{i-1}) = ya; z <- z + dz + dt/6 k4.  The tile's share of
+// z_u . gh (NaN terms skipped) goes to partial[tile] (cu-G:1457-1483).
+template <int E, int TX, int TY, int NT, int MODE>
+__device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, double* __restrict__ Zs,
+                                          const double* __restrict__ Z0, double* __restrict__ D,
+                                          const uint8_t* __restrict__ wc, const double* __restrict__ ys,
+                                          long long off, double cZ, double cD, double* __restrict__ out,
+                                          const double* __restrict__ ghs, double& zgh) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
+    constexpr int IT = (N + NT - 1) / NT;
+    constexpr int IN = TX * TY;
+    double ku[IT], kv[IT], kw[IT];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = threadIdx.x + it * NT;
+        if (q < N) {
+            const int r = HALO - E + q / W, c = HALO - E + q % W;
+            const int s = r * RW + c;
+            const long long o = off + (long long)r * g.ld + c;
+            const int code = __ldg(wc + o);
+            if (isnan(Zs[s])) {
+                ku[it] = kv[it] = kw[it] = __longlong_as_double(0x7ff8000000000000LL);
+            } else {
+                const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+                adj_at<RW, RN>(P, Zs, s, code, J, ku[it], kv[it], kw[it]);
+            }
+        }
+    }
+    if (MODE != 2) __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = threadIdx.x + it * NT;
+        if (q < N) {
+            const int r = HALO - E + q / W, c = HALO - E + q % W;
+            const int s = r * RW + c;
+            const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+            const int d = (r - HALO) * TX + (c - HALO);
+            if (MODE == 2) {
+                const long long o = (long long)r * g.ld + c;
+                const double nu = (Z0[s] + D[d]) + cD * ku[it];
+                out[o] = nu;
+                out[g.plane + o] = (Z0[RN + s] + D[IN + d]) + cD * kv[it];
+                out[2 * g.plane + o] = (Z0[2 * RN + s] + D[2 * IN + d]) + cD * kw[it];
+                const double t = nu * __ldg(ghs + o);
+                if (!isnan(t)) zgh += t;
+            } else {
+                Zs[s] = Z0[s] + cZ * ku[it];
+                Zs[RN + s] = Z0[RN + s] + cZ * kv[it];
+                Zs[2 * RN + s] = Z0[2 * RN + s] + cZ * kw[it];
+                if (inner) {
+                    if (MODE == 0) {
+                        D[d] = cD * ku[it];
+                        D[IN + d] = cD * kv[it];
+                        D[2 * IN + d] = cD * kw[it];
+                    } else {
+                        D[d] = D[d] + cD * ku[it];
+                        D[IN + d] = D[IN + d] + cD * kv[it];
+                        D[2 * IN + d] = D[2 * IN + d] + cD * kw[it];
+                    }
+                }
+            }
+        }
+    }
+    if (MODE != 2) __syncthreads();
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z,
+                                                 double* __restrict__ zout, const double* __restrict__ yb,
+                                                 const double* __restrict__ yh, const double* __restrict__ ya,
+                                                 const uint8_t* __restrict__ wc, const double* __restrict__ gh,
+                                                 double* __restrict__ partial) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    constexpr int IN = TX * TY;
+    extern __shared__ double4 smem_raw[];
+    double* Zs = reinterpret_cast<double*>(smem_raw);
+    double* Z0 = Zs + 3 * RN;
+    double* D = Z0 + 3 * RN;
+    double* red = D + 3 * IN;
+    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const long long off = (long long)i0 * g.ld + j0;
+    const bool vec_ok = ((g.ld | j0) & 1) == 0;
+    load_region<RH, RW, NT>(Zs, z + off, g.ld, g.plane, vec_ok);
+    __syncthreads();
+    for (int q = threadIdx.x; q < 3 * RN; q += NT) Z0[q] = Zs[q];
+    __syncthreads();
+    const double dt = P.dt;
+    double zgh = 0.0;
+    const uint8_t* wco = wc;  // byte codes, same padded layout (plane-less)
+    adj_stage<3, TX, TY, NT, 0>(P, g, Zs, Z0, D, wco, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, nullptr, zgh);
+    adj_stage<2, TX, TY, NT, 1>(P, g, Zs, Z0, D, wco, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, nullptr, zgh);
+    adj_stage<1, TX, TY, NT, 1>(P, g, Zs, Z0, D, wco, yh, off, dt, 2.0 / 6.0 * dt, nullptr, nullptr, zgh);
+    adj_stage<0, TX, TY, NT, 2>(P, g, Zs, Z0, D, wco, ya, off, 0.0, 1.0 / 6.0 * dt, zout + off, gh + off, zgh);
+    const double s = block_sum<NT>(zgh, red);
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// z_u . gh over one tile (NaN terms skipped) -> partial[tile].
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_dot_gh(DevGrid g, const double* __restrict__ z,
+                                               const double* __restrict__ gh, double* __restrict__ partial) {
+    __shared__ double red[NT / 32];
+    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < TX * TY; q += NT) {
+        const int r = q / TX, c = q % TX;
+        const long long o = (long long)(i0 + HALO + r) * g.ld + (j0 + HALO + c);
+        const double t = z[o] * gh[o];
+        if (!isnan(t)) acc += t;
+    }
+    const double s = block_sum<NT>(acc, red);
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// out[row] = sum_k partial[row*ntiles + k], fixed order (one block per row).
+__global__ void k_sum_rows(const double* __restrict__ partial, int ntiles, double* __restrict__ out) {
+    __shared__ double red[8];
+    const double* p = partial + (long long)blockIdx.x * ntiles;
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < ntiles; k += 256) acc += p[k];
+    const double s = block_sum<256>(acc, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+// ----------------------------------------------------------- layout kernels
+
+// Compact [u;v;w] (n_num each, scaled by `scale`) -> padded NaN grid.
+__global__ void k_scatter(DevGrid g, const double* __restrict__ yc, int n_num,
+                          const long long* __restrict__ pos, double scale, double* __restrict__ y) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_num) return;
+    const long long o = pos[m];
+    y[o] = yc[m] * scale;
+    y[g.plane + o] = yc[n_num + m] * scale;
+    y[2 * g.plane + o] = yc[2 * n_num + m] * scale;
+}
+
+// Padded grid -> compact [u;v;w].
+__global__ void k_gather(DevGrid g, const double* __restrict__ y, int n_num,
+                         const long long* __restrict__ pos, double* __restrict__ yc) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_num) return;
+    const long long o = pos[m];
+    yc[m] = y[o];
+    yc[n_num + m] = y[g.plane + o];
+    yc[2 * n_num + m] = y[2 * g.plane + o];
+}
+
+// Objective at T: for each field f, zc_f = -gamma_f * (S y_f) with S in CSR
+// (row sums in ascending column order, the order of the reference's CSC
+// accumulation, cu-G:1514-1522); per-block partials of y_f . zc_f.
+__global__ void k_objective(const double* __restrict__ yc, int n_num, const long long* __restrict__ rowptr,
+                            const int* __restrict__ colidx, const double* __restrict__ val, double g0,
+                            double g1, double g2, double* __restrict__ zc, double* __restrict__ partial) {
+    __shared__ double red[8];
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    double acc = 0.0;
+    if (r < n_num) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (long long k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+            const int c = colidx[k];
+            const double a = val[k];
+            s0 += a * yc[c];
+            s1 += a * yc[n_num + c];
+            s2 += a * yc[2 * n_num + c];
+        }
+        const double z0 = s0 * -g0, z1 = s1 * -g1, z2 = s2 * -g2;
+        zc[r] = z0;
+        zc[n_num + r] = z1;
+        zc[2 * n_num + r] = z2;
+        acc = (yc[r] * z0 + yc[n_num + r] * z1) + yc[2 * n_num + r] * z2;
+    }
+    const double s = block_sum<256>(acc, red);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------- launchers
+
+template <int TX, int TY, int NT>
+static size_t fwd_smem() {
+    constexpr int RN = (TX + 2 * HALO) * (TY + 2 * HALO);
+    return sizeof(double) * (6 * RN + 3 * TX * TY);
+}
+template <int TX, int TY, int NT>
+static size_t mid_smem() {
+    constexpr int RN = (TX + 4) * (TY + 4);
+    return sizeof(double) * (9 * RN);
+}
+template <int TX, int TY, int NT>
+static size_t adj_smem() {
+    constexpr int RN = (TX + 2 * HALO) * (TY + 2 * HALO);
+    return sizeof(double) * (6 * RN + 3 * TX * TY + NT / 32);
+}
+
+template <int TX, int TY, int NT>
+static cudaError_t setup_tile() {
+    cudaError_t e;
+    e = cudaFuncSetAttribute(k_fwd_step<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem<TX, TY, NT>());
+    if (e) return e;
+    e = cudaFuncSetAttribute(k_adj_mid<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid_smem<TX, TY, NT>());
+    if (e) return e;
+    return cudaFuncSetAttribute(k_adj_step<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem<TX, TY, NT>());
+}
+
+#define FKADJ_TILES(X) X(32, 32, 256) X(32, 16, 256) X(64, 32, 512) X(16, 16, 256)
+
+int tile_count() { return 4; }
+
+TileShape tile_shape(int t) {
+    switch (t) {
+        case 1: return {32, 16, 256};
+        case 2: return {64, 32, 512};
+        case 3: return {16, 16, 256};
+        default: return {32, 32, 256};
+    }
+}
+
+cudaError_t kernels_init() {
+    cudaError_t e;
+#define X(a, b, c) if ((e = setup_tile<a, b, c>()) != cudaSuccess) return e;
+    FKADJ_TILES(X)
+#undef X
+    return cudaSuccess;
+}
+
+#define DISPATCH(tile, CALL)                                           \
+    switch (tile) {                                                    \
+        case 1: { constexpr int TX = 32, TY = 16, NT = 256; CALL; } break; \
+        case 2: { constexpr int TX = 64, TY = 32, NT = 512; CALL; } break; \
+        case 3: { constexpr int TX = 16, TY = 16, NT = 256; CALL; } break; \
+        default: { constexpr int TX = 32, TY = 32, NT = 256; CALL; } break; \
+    }
+
+static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
+    return dim3((g.ncols + tx - 1) / tx, (g.nrows + ty - 1) / ty);
+}
+
+cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
+                            const double* gh, double E0, double Eh, double E1, cudaStream_t st) {
+    DISPATCH(tile, (k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, fwd_smem<TX, TY, NT>(), st>>>(
+                        P, g, yin, yout, gh, E0, Eh, E1)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
+                           const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
+                           cudaStream_t st) {
+    DISPATCH(tile, (k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, TY), NT, mid_smem<TX, TY, NT>(), st>>>(
+                        P, g, ya, yb, gh, yh, Ea, Eb, E3, hw)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
+                            const double* yb, const double* yh, const double* ya, const uint8_t* wc,
+                            const double* gh, double* partial, cudaStream_t st) {
+    DISPATCH(tile, (k_adj_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, adj_smem<TX, TY, NT>(), st>>>(
+                        P, g, z, zout, yb, yh, ya, wc, gh, partial)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dot_gh(int tile, const DevGrid& g, const double* z, const double* gh, double* partial,
+                          cudaStream_t st) {
+    DISPATCH(tile, (k_dot_gh<TX, TY, NT><<<tile_grid(g, TX, TY), NT, 0, st>>>(g, z, gh, partial)));
+    return cudaGetLastError();
+}
+
+int tiles_of(int tile, const DevGrid& g) {
+    const TileShape t = tile_shape(tile);
+    return ((g.ncols + t.tx - 1) / t.tx) * ((g.nrows + t.ty - 1) / t.ty);
+}
+
+cudaError_t launch_sum_rows(const double* partial, int rows, int ntiles, double* out, cudaStream_t st) {
+    if (rows <= 0) return cudaSuccess;
+    k_sum_rows<<<rows, 256, 0, st>>>(partial, ntiles, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const DevGrid& g, const double* yc, int n_num, const long long* pos, double scale,
+                           double* y, cudaStream_t st) {
+    k_scatter<<<(n_num + 255) / 256, 256, 0, st>>>(g, yc, n_num, pos, scale, y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather(const DevGrid& g, const double* y, int n_num, const long long* pos, double* yc,
+                          cudaStream_t st) {
+    k_gather<<<(n_num + 255) / 256, 256, 0, st>>>(g, y, n_num, pos, yc);
+    return cudaGetLastError();
+}
+
+int objective_blocks(int n_num) { return (n_num + 255) / 256; }
+
+cudaError_t launch_objective(const double* yc, int n_num, const long long* rowptr, const int* colidx,
+                             const double* val, const double gamma[3], double* zc, double* partial,
+                             cudaStream_t st) {
+    k_objective<<<objective_blocks(n_num), 256, 0, st>>>(yc, n_num, rowptr, colidx, val, gamma[0], gamma[1],
+                                                         gamma[2], zc, partial);
+    return cudaGetLastError();
+}
+
+}  // namespace fkadj

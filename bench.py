@@ -1,0 +1,301 @@
+#!/usr/bin/env python3
+"""Benchmark: forward + adjoint gradients per second at 512^2 on B200.
+
+Workload (one "step" = one gradient): 512 x 512 FK grid (fp64), dx 0.025 cm,
+dt 0.02 ms, 20000 RK4 steps, 200 circular holes, 8 broken wavefronts, E(t)
+piecewise constant over 400 intervals, J = mean u(T)^2, reference-mode
+adjoint with sqrt(nt) checkpoints (142 stored states + 141-state segment
+buffer recomputed backward).  Seeded synthetic inputs with the reference's
+layouts (the reference publishes no benchmark).
+
+  value   gradients/s with the inputs resident on the device, device time
+          (CUDA events on the engine's stream), max over ranks, x ranks
+  e2e     the same metric through the drop-in C-ABI call fkadj_grad with host
+          buffers (pinned), host<->device copies inside the timed region
+  roofline  the dominant kernel's algorithmic bytes / its average launch time
+          (sampled CUDA events inside the engine, same process, right after
+          the timed region) against MEASURED_PEAKS.json's HBM copy bandwidth
+  cpu_baseline  the CPU oracle (C, OpenMP, all host cores) on a bounded
+          sample of the same workload, scaled to gradients/s
+
+--impl reference times the reference algorithm on the host cores (the CPU
+oracle port; the reference's own code runs through MATLAB, absent here).
+Multi-GPU: independent replicas (one instance per rank, no collective on the
+data path); torch.distributed/NCCL only for the barrier and the max.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "adjoint-optimization_b200")
+for _p in (PKG, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "fwd+adjoint gradients/s at 512^2"
+UNIT = "gradients/s"
+
+# algorithmic bytes per dense cell per launch (one RK4 step of the unit)
+BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
+                  1: 80.0,    # adjoint midpoint: read y_i, y_{i-1} (48) + gh (8), write yh (24)
+                  2: 128.0}   # adjoint step: read z, y_i, yh, y_{i-1} (96) + gh (8), write z (24)
+KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(args):
+    from fkadj import workloads as W
+    inst = W.large_instance(n=args.n, nt=args.nt, seed=1)
+    return inst
+
+
+def workload_config(args, inst, ckpt):
+    return {"workload": f"FK {args.n}x{args.n} fp64, {args.nt} RK4 steps, 200 holes, 8 wavefronts, "
+                        f"400 E intervals, J=mean u^2, ref-mode adjoint, {ckpt} checkpoints",
+            "grid": [args.n, args.n], "nt": args.nt, "dt_ms": inst.dt, "dx_cm": inst.dx,
+            "active_cells": inst.n_num, "checkpoint": ckpt, "grad_mode": "ref",
+            "l2": "working set larger than L2 (checkpoint + segment store > 1 GB per gradient)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def cpu_sample(args, inst):
+    """CPU oracle (reference algorithm, FP64, OpenMP on all host cores) on a
+    bounded sample: the same grid for args.cpu_steps steps, scaled to nt."""
+    import numpy as np
+    import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    nts = args.cpu_steps
+    Et = np.ascontiguousarray(inst.Et[:nts + 1])
+    obj = O.Objective(inst.S, inst.gamma)
+    t0 = time.perf_counter()
+    O.grad(inst.params, inst.dt, Et, nts, inst.nrows, inst.ncols, inst.y0_grid, inst.gh_grid,
+           inst.active_index, obj, inst.alpha, mode="ref")
+    dt = time.perf_counter() - t0
+    per_grad = dt * inst.nt / nts
+    return {"value": 1.0 / per_grad, "unit": UNIT, "cores": O.threads(), "kind": "port",
+            "sample": f"{inst.nrows}x{inst.ncols} grid, {nts} fwd+adjoint steps ({dt:.1f} s) scaled to "
+                      f"{inst.nt} steps; C oracle, OpenMP"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    inst = workload(args)
+    for _ in range(args.warmup):
+        pass
+    vals = [cpu_sample(args, inst) for _ in range(max(1, args.steps if args.steps <= 2 else 2))]
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[0])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args, inst, "full (host)"), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from fkadj import _lib, api
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def gmax(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    inst = workload(args)
+    ckpt = {"sqrt": _lib.CKPT_SQRT, "full": _lib.CKPT_FULL, "auto": _lib.CKPT_AUTO}[args.ckpt]
+    stream = torch.cuda.Stream()
+    opts = api.options(ckpt_policy=ckpt, stream=stream.cuda_stream, device=local, tile=args.tile)
+    pb = api.Problem(inst, opts=opts)
+    Et = np.ascontiguousarray(inst.Et)
+    pb.grad(Et, inst.y0)                     # uploads the initial state (resident afterwards)
+    for _ in range(max(0, args.warmup - 1)):
+        pb.grad(Et)
+    launches = 0
+    clk = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        pb.grad(Et)
+        launches += pb.last_launches
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier()
+    ms = gmax(ev0.elapsed_time(ev1))
+    value = world * args.steps / (ms / 1000.0)
+
+    # roofline: sampled per-kernel device times in one more gradient
+    pb.set_profiling(True)
+    pb.grad(Et)
+    pb.set_profiling(False)
+    recompute = 0 if args.ckpt == "full" else inst.nt - (inst.nt + pb_stride(inst.nt) - 1) // pb_stride(inst.nt)
+    per_grad = {0: inst.nt + recompute, 1: inst.nt, 2: inst.nt}
+    kt = {k: pb.kernel_time(k) for k in (0, 1, 2)}
+    share = {k: kt[k][0] * per_grad[k] for k in kt}
+    dom = max(share, key=share.get)
+    cells = inst.nrows * inst.ncols
+    avg_ms = kt[dom][0]
+    achieved = BYTES_PER_CELL[dom] * cells / (avg_ms / 1000.0) / 1e9
+    peak, peak_kind = peaks()
+    roof = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": args.traffic,
+            "bytes_per_launch": BYTES_PER_CELL[dom] * cells, "avg_launch_ms": avg_ms,
+            "samples": kt[dom][1],
+            "kernel_ms": {KERNEL_NAMES[k]: kt[k][0] for k in kt},
+            "time_share": {KERNEL_NAMES[k]: share[k] / sum(share.values()) for k in share},
+            "note": "FP64-arithmetic bound (3 tanh per vector-field evaluation); "
+                    "HBM fraction reported against the copy peak"}
+    pb.close()
+
+    # e2e through the drop-in C ABI (fkadj_grad), host buffers in pinned memory
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    Et_h, y0_h = pin(inst.Et), pin(inst.y0)
+    ai_h, gh_h = pin(inst.active_index.astype(np.int32)), pin(inst.ghost.astype(np.float64))
+    import scipy.sparse as sp
+    S = sp.csc_matrix(inst.S)
+    h2d = Et_h.nbytes + y0_h.nbytes + ai_h.nbytes + gh_h.nbytes + 24 + S.indptr.size * 8 + S.indices.size * 8 \
+        + S.data.size * 8
+    d2h = (inst.nt + 1) * 8 + 3 * 8
+    eopts = api.options(ckpt_policy=ckpt, device=local, tile=args.tile)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        api.fk_grad_Et(Et_h, inst.dt, inst.nt, y0_h, ai_h, inst.ncols, inst.nrows, gh_h, inst.gamma, S,
+                       inst.alpha, params=inst.params, opts=eopts)
+    torch.cuda.synchronize()
+    e2e_s = gmax(time.perf_counter() - t0)
+    e2e = {"value": world * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+           "path": "fkadj_grad (drop-in for fk_grad_Et_comp), one call per gradient incl. device setup"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(args, inst)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": workload_config(args, inst, args.ckpt), "roofline": roof, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def pb_stride(nt):
+    import math
+    return max(2, int(math.ceil(math.sqrt(nt))))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fkadj", choices=["fkadj", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--nt", type=int, default=20000)
+    ap.add_argument("--ckpt", default="sqrt", choices=["sqrt", "full", "auto"])
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--cpu-steps", type=int, default=24)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu dram bytes per launch of the dominant kernel, if captured")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

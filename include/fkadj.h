@@ -1,0 +1,163 @@
+/*
+ * fkadj.h -- C ABI of libfkadj, a B200 (sm_100a) Fenton-Karma forward /
+ * adjoint engine.  Plain pointers and sizes only; every entry point returns
+ * an fkadj_status and never exits the process.
+ *
+ * It is the drop-in seam behind the reference's two MEX gateways
+ * (agarzon27/adjoint-optimization):
+ *   fkadj_forward  replaces  fk_forward_Et_comp
+ *                  (decl src/cuda/fk_forward_Et_param_mex.cpp:27-29,
+ *                   def  src/cuda/fk_forward_Et_mono_PARAMETERS.cu:646-849)
+ *   fkadj_grad     replaces  fk_grad_Et_comp
+ *                  (decl src/cuda/fk_grad_Et_param_mex.cpp:3-6,
+ *                   def  src/cuda/fk_grad_Et_mono_PARAMETERS.cu:1569-1938)
+ * with the same argument meaning and layouts:
+ *   Et[nt+1]          E sample i at t = i*dt
+ *   y_ini[3*n_num]    compact active cells in increasing linear index, [u;v;w]
+ *   active_index[n]   n = nrows*ncols, linear index k = i*ncols + j,
+ *                     1-based compact index, 0 = hole
+ *   gh_num[n_num]     ghost_lr (-1/0/+1 for the shipped grids); the source is
+ *                     E(t) * (Du*2/h) * gh_num on u
+ *   S                 n_num x n_num objective matrix in CSC (Jc, Ir, Sv)
+ *   ys[ns][3n], yf[3n] dense grids with NaN at holes
+ * Differences (all additive): the FK parameter set is a runtime argument
+ * (the reference compiles it in, src/cuda/fk_parameters_00_05_alpha_0p8_dx_0p035.h),
+ * the CSC matrix replaces the mxArray, and an optional options struct selects
+ * the gradient mode, the trajectory checkpoint policy and the CUDA stream.
+ * The reference's param_str output is returned by fkadj_param_string.
+ */
+#ifndef FKADJ_H
+#define FKADJ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FKADJ_ABI_VERSION 1
+
+typedef enum {
+    FKADJ_OK = 0,
+    FKADJ_ERR_ARG = 1,        /* invalid argument (sizes, null pointers, mismatch) */
+    FKADJ_ERR_CUDA = 2,       /* a CUDA runtime call failed; see fkadj_last_error */
+    FKADJ_ERR_NOMEM = 3,      /* device or host allocation failed */
+    FKADJ_ERR_NUMERIC = 4,    /* non-finite value in an active cell */
+    FKADJ_ERR_NODEVICE = 5,   /* no CUDA device / kernels not loadable */
+    FKADJ_ERR_BUSY = 6,       /* serving queue full */
+    FKADJ_ERR_TIMEOUT = 7     /* bounded wait expired */
+} fkadj_status;
+
+/* FK constants, diffusivities and spacing h (cm).  Field order and meaning
+ * of src/cuda/fk_parameters_00_05_alpha_0p8_dx_0p035.h:2-23. */
+typedef struct {
+    double u_c, u_v, tau_d, tau_v1_minus, tau_v2_minus, tau_v_plus, tau_0, tau_r,
+           tau_si, u_csi, k_fk, tau_w_minus, tau_w_plus, Du, Dv, Dw, ksm, h;
+} fkadj_params;
+
+typedef enum {
+    FKADJ_GRAD_REF = 0,   /* the reference's continuous adjoint: Hermite midpoint
+                             states, backward RK4 on -dz/dt = (L+J_F)^T z;
+                             gradE[i] = alpha*Et[i] - z(t_i).gh  (cu-G:1924-1926) */
+    FKADJ_GRAD_EXACT = 1  /* discrete adjoint of the RK4 sweep and of the
+                             not-a-knot spline; gradE[i] = (1/dt) dLcost/dEt[i] */
+} fkadj_grad_mode;
+
+typedef enum {
+    FKADJ_CKPT_AUTO = 0,     /* FULL when it fits the budget, else SQRT, else BINOMIAL */
+    FKADJ_CKPT_FULL = 1,     /* every state resident on the device */
+    FKADJ_CKPT_SQRT = 2,     /* ~sqrt(nt) checkpoints, segments recomputed backward */
+    FKADJ_CKPT_BINOMIAL = 3  /* binomial (revolve) schedule within ckpt_budget_bytes */
+} fkadj_ckpt_policy;
+
+typedef struct {
+    int grad_mode;              /* fkadj_grad_mode (default FKADJ_GRAD_REF) */
+    int ckpt_policy;            /* fkadj_ckpt_policy (default AUTO) */
+    int64_t ckpt_budget_bytes;  /* device bytes for stored states; 0 = 60% of free */
+    int device;                 /* CUDA device ordinal; -1 = current */
+    void *stream;               /* cudaStream_t to run on; NULL = library stream */
+    int tile;                   /* kernel tile preset (0 = autotuned default) */
+    int verbose;                /* 0 = silent */
+} fkadj_options;
+
+/* Fills *opt with the defaults. */
+void fkadj_default_options(fkadj_options *opt);
+/* The reference's default FK parameter set (the header above) with h = dx. */
+void fkadj_default_params(fkadj_params *p, double dx);
+
+/* Forward sweep (replaces fk_forward_Et_comp, cu-F:646-849).  Writes state
+ * snapshots every nstep steps into ys (ns of them, the final step excluded when
+ * nt/nstep is an integer, as compute_ns does in fk_forward_Et_param_mex.cpp:7-25)
+ * and the final state into yf.  ys may be NULL when ns == 0. */
+fkadj_status fkadj_forward(const fkadj_params *p, double dt, const double *Et, int nt,
+                           const double *y_ini, const int *active_index, int nrows,
+                           int ncols, int n_num, const double *gh_num, int nstep, int ns,
+                           double *ys, double *yf, const fkadj_options *opt);
+
+/* Objective and gradient (replaces fk_grad_Et_comp, cu-G:1569-1938):
+ * L0 = sum_v gamma[v] y_v(T)^T S y_v(T), LE = dt*sum Et^2,
+ * Lcost = L0/2 + alpha*LE/2, gradE[nt+1].  yf (may be NULL) receives the
+ * final forward state (dense NaN grid). */
+fkadj_status fkadj_grad(const fkadj_params *p, double dt, const double *Et, int nt,
+                        const double *y_ini, const int *active_index, int nrows, int ncols,
+                        int n_num, const double *gh_num, const double *gamma,
+                        int64_t S_ncol, const int64_t *S_colptr, const int64_t *S_rowidx,
+                        const double *S_val, double alpha, double *L0, double *LE,
+                        double *Lcost, double *gradE, double *yf, const fkadj_options *opt);
+
+/* Parameter provenance text (the role of the reference's param_str).  The
+ * returned string is owned by the library and valid until the next call from
+ * the same thread. */
+const char *fkadj_param_string(const fkadj_params *p);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *fkadj_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Resident problems: geometry, objective and work buffers stay on the device
+ * between calls (optimisation loops, line-search probes, serving).
+ * --------------------------------------------------------------------- */
+typedef struct fkadj_problem fkadj_problem;
+
+fkadj_status fkadj_problem_create(fkadj_problem **out, const fkadj_params *p, double dt, int nt,
+                                  const int *active_index, int nrows, int ncols, int n_num,
+                                  const double *gh_num, const double *gamma, int64_t S_ncol,
+                                  const int64_t *S_colptr, const int64_t *S_rowidx,
+                                  const double *S_val, double alpha, const fkadj_options *opt);
+void fkadj_problem_destroy(fkadj_problem *pb);
+
+/* Device bytes the problem holds (geometry + work + trajectory store). */
+int64_t fkadj_problem_device_bytes(const fkadj_problem *pb);
+
+/* Objective only (forward sweep, no trajectory storage). */
+fkadj_status fkadj_problem_objective(fkadj_problem *pb, const double *Et, const double *y_ini,
+                                     double *L0, double *LE, double *Lcost, double *yf);
+
+/* Objective + gradient through the problem's buffers.  In both calls y_ini
+ * may be NULL to re-use the initial state of the previous call, which stays
+ * resident on the device. */
+fkadj_status fkadj_problem_grad(fkadj_problem *pb, const double *Et, const double *y_ini,
+                                double *L0, double *LE, double *Lcost, double *gradE,
+                                double *yf);
+
+/* Timing of the last call on the problem, milliseconds of device time:
+ * out[0] forward, out[1] backward (incl. recompute), out[2] total. */
+void fkadj_problem_last_timing(const fkadj_problem *pb, double out[3]);
+
+/* Number of kernel launches the last call on the problem issued. */
+int64_t fkadj_problem_last_launches(const fkadj_problem *pb);
+
+/* Sampled per-kernel device time: when enabled, CUDA events bracket about one
+ * in (nt/100) launches of each kernel kind during the following calls.
+ * kernel: 0 forward step, 1 adjoint midpoint, 2 adjoint step.  Reports the
+ * average milliseconds per launch of the last call and the sample count.
+ * No reference counterpart (the reference has no timers besides tic/toc in
+ * src/cuda/simple_grad_desc.m:80-86). */
+void fkadj_problem_set_profiling(fkadj_problem *pb, int enable);
+void fkadj_problem_kernel_time(const fkadj_problem *pb, int kernel, double *avg_ms, int64_t *samples);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FKADJ_H */

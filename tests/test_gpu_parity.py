@@ -1,0 +1,107 @@
+"""CUDA path vs the CPU oracle on the same seeded inputs (through the C ABI).
+
+Tolerances: states 1e-10 relative (max-norm, at horizons short enough that
+round-off growth stays below it), J and gradE 1e-8 relative (2-norm); the
+golden 256^2 x 3000-step gradient of the reference to 1e-9 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from fkadj import api, geometry as G, workloads as W
+from fkadj import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    m = np.isfinite(b)
+    assert np.array_equal(np.isfinite(a), m), "NaN pattern differs"
+    return np.abs(a[m] - b[m]).max() / max(np.abs(b[m]).max(), 1e-300)
+
+
+def _inst(n=64, nt=200, seed=11, ncols=None, **kw):
+    return W.make_instance(n, nt, seed=seed, ncols=ncols, n_obstacles=kw.pop("n_obstacles", 6), **kw)
+
+
+@pytest.mark.parametrize("shape", [(64, 64), (48, 80), (50, 70), (33, 129)])
+def test_forward_matches_oracle(shape):
+    nr, nc = shape
+    inst = _inst(nr, 150, seed=nr * 7 + nc, ncols=nc)
+    ys, yf, pstr = api.fk_forward_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols,
+                                     inst.nrows, inst.ghost, 50, params=inst.params)
+    ns = api.compute_ns(inst.nt, 50)
+    ys_o, yf_o = O.forward(inst.params, inst.dt, inst.Et, inst.nt, nr, nc, inst.y0_grid, inst.gh_grid,
+                           50, ns)
+    assert _rel(yf, yf_o) <= 1e-10
+    assert ys.shape == (3 * nr * nc, ns)
+    for k in range(ns):
+        assert _rel(ys[:, k], ys_o[k]) <= 1e-10
+    assert "h = 0.025" in pstr
+
+
+@pytest.mark.parametrize("tile", [0, 1, 2, 3])
+def test_forward_state_is_independent_of_tile_shape(tile):
+    inst = _inst(96, 40, seed=3, ncols=72)
+    ref = api.fk_forward_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                            inst.ghost, 40, params=inst.params, opts=api.options(tile=0))[1]
+    yf = api.fk_forward_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                           inst.ghost, 40, params=inst.params, opts=api.options(tile=tile))[1]
+    assert np.array_equal(np.isnan(ref), np.isnan(yf))
+    assert np.array_equal(ref[~np.isnan(ref)], yf[~np.isnan(yf)])
+
+
+@pytest.mark.parametrize("objective", ["mean_u2", "gradient"])
+def test_ref_gradient_matches_oracle(objective):
+    inst = _inst(64, 120, seed=21, objective=objective, ncols=80)
+    alpha = 0.3
+    g, Lc, L0, LE, _, yf = api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols,
+                                          inst.nrows, inst.ghost, inst.gamma, inst.S, alpha,
+                                          params=inst.params, return_yf=True)
+    obj = O.Objective(inst.S, inst.gamma)
+    r = O.grad(inst.params, inst.dt, inst.Et, inst.nt, inst.nrows, inst.ncols, inst.y0_grid, inst.gh_grid,
+               inst.active_index, obj, alpha, mode="ref")
+    assert _rel(yf, r["yf"]) <= 1e-10
+    assert abs(L0 - r["L0"]) <= 1e-10 * abs(r["L0"])
+    assert abs(LE - r["LE"]) <= 1e-13 * abs(r["LE"])
+    assert abs(Lc - r["Lcost"]) <= 1e-10 * abs(r["Lcost"])
+    assert np.linalg.norm(g - r["gradE"]) <= 1e-8 * np.linalg.norm(r["gradE"])
+
+
+def test_sqrt_checkpointing_equals_full_storage():
+    inst = _inst(64, 150, seed=5)
+    args = (inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows, inst.ghost,
+            inst.gamma, inst.S, 0.0)
+    full = api.fk_grad_Et(*args, params=inst.params, opts=api.options(ckpt_policy=_lib.CKPT_FULL))
+    sq = api.fk_grad_Et(*args, params=inst.params, opts=api.options(ckpt_policy=_lib.CKPT_SQRT))
+    assert np.array_equal(full[0], sq[0])
+    assert full[1] == sq[1]
+
+
+def test_golden_reference_gradient(golden):
+    """The reference's shipped 256^2 x 3000-step gradient (GD iteration 50)."""
+    k = 0
+    ai = golden["active_index"]
+    n = int(golden["nrows"])
+    mask = (ai > 0).reshape(n, n)
+    S = G.objective_matrix(mask)
+    from fkadj.params import FkParams
+    P = FkParams().with_h(float(golden["h"]))
+    g, Lc, L0, LE, _ = api.fk_grad_Et(golden["Et"][k], float(golden["dt"]), int(golden["nt"]), golden["y0"],
+                                      ai, n, n, golden["ghost_lr"].astype(float), golden["gamma"], S,
+                                      float(golden["alpha"]), params=P)
+    ge = golden["gradE"][k]
+    assert abs(Lc - golden["Lcost"][k]) <= 1e-10 * abs(golden["Lcost"][k])
+    assert np.linalg.norm(g - ge) <= 1e-9 * np.linalg.norm(ge)
+
+
+def test_problem_handle_repeated_calls_are_deterministic():
+    inst = _inst(64, 100, seed=8)
+    with api.Problem(inst) as pb:
+        a = pb.grad(inst.Et, inst.y0)
+        b = pb.grad(inst.Et, inst.y0)
+        o = pb.objective(inst.Et, inst.y0)
+        assert pb.last_launches > 0
+        assert pb.device_bytes > 0
+    assert np.array_equal(a["gradE"], b["gradE"])
+    assert a["Lcost"] == b["Lcost"] == o["Lcost"]
