@@ -35,21 +35,34 @@ struct DevGrid {
     long long plane;  // doubles per field plane
 };
 
-// Ionic currents (formula of cu-F:29-45).
+// Smoothed step s = (1 + tanh x)/2 written as the logistic 1/(1 + e^{-2x})
+// (the same function; one exp and one reciprocal instead of a tanh) and its
+// complement 1 - s = e^{-2x} s without cancellation.  e^{-2x} overflows to
+// +inf for x < -354 and gives s = 0, 1 - s = 1 as tanh does.
+struct Step {
+    double s, c;  // s and 1 - s
+};
+__device__ __forceinline__ Step smooth_step(double x) {
+    const double e = exp(-2.0 * x);
+    const double s = 1.0 / (1.0 + e);
+    return {s, isinf(e) ? 1.0 : e * s};
+}
+
+// Ionic currents (formula of cu-F:29-45): p, q and (1 + tanh)/2 of the slow
+// inward current are the three smoothed steps.
 __device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, double w,
                                        double& ud, double& vd, double& wd) {
-    const double tc = tanh(P.ksm * (u - P.u_c));
-    const double tv = tanh(P.ksm * (u - P.u_v));
-    const double ts = tanh(P.k_fk * (u - P.u_csi));
-    const double p = 0.5 * (1.0 + tc);
-    const double q = 0.5 * (1.0 + tv);
+    const Step sp = smooth_step(P.ksm * (u - P.u_c));
+    const Step sq = smooth_step(P.ksm * (u - P.u_v));
+    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
+    const double p = sp.s, q = sq.s;
     const double j_fi = -v * p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
-    const double j_so = u * (1.0 - p) * P.r_tau_0 + p * P.r_tau_r;
-    const double tvm = q * P.tau_v1m + (1.0 - q) * P.tau_v2m;
-    const double j_si = -w * (1.0 + ts) * P.r_2tau_si;
+    const double j_so = u * sp.c * P.r_tau_0 + p * P.r_tau_r;
+    const double tvm = q * P.tau_v1m + sq.c * P.tau_v2m;
+    const double j_si = -w * (2.0 * ss.s) * P.r_2tau_si;
     ud = -(j_fi + j_so + j_si);
-    vd = ((1.0 - p) * (1.0 - v)) / tvm - (p * v) * P.r_tau_vp;
-    wd = ((1.0 - p) * (1.0 - w)) * P.r_tau_wm - (p * w) * P.r_tau_wp;
+    vd = (sp.c * (1.0 - v)) / tvm - (p * v) * P.r_tau_vp;
+    wd = (sp.c * (1.0 - w)) * P.r_tau_wm - (p * w) * P.r_tau_wp;
 }
 
 // The seven non-zero entries of the transposed Jacobian of fk_ion
@@ -59,28 +72,29 @@ struct JacT {
     double a0, a1, a2, a3, a4, a5, a6;
 };
 
+// 1 - tanh^2 = 4 s (1 - s) for the smoothed step s.
 __device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, double w) {
-    const double tc = tanh(P.ksm * (u - P.u_c));
-    const double tv = tanh(P.ksm * (u - P.u_v));
-    const double ts = tanh(P.k_fk * (u - P.u_csi));
-    const double p = 0.5 * tc + 0.5;
-    const double q = 0.5 * tv + 0.5;
-    const double dp = 1.0 - tc * tc;
-    const double dq = 1.0 - tv * tv;
-    const double tvm = q * P.tau_v1m + P.tau_v2m * (1.0 - q);
+    const Step sp = smooth_step(P.ksm * (u - P.u_c));
+    const Step sq = smooth_step(P.ksm * (u - P.u_v));
+    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
+    const double p = sp.s, q = sq.s;
+    const double dp = 4.0 * sp.s * sp.c;
+    const double dq = 4.0 * sq.s * sq.c;
+    const double ds = 4.0 * ss.s * ss.c;
+    const double tvm = q * P.tau_v1m + P.tau_v2m * sq.c;
     const double rtvm = 1.0 / tvm;
     const double hk = 0.5 * dp * P.ksm;
     JacT J;
     J.a0 = -hk * P.r_tau_r + hk * v * (1.0 - u) * (u - P.u_c) * P.r_tau_d + hk * u * P.r_tau_0 +
-           P.k_fk * w * (1.0 - ts * ts) * P.r_2tau_si + p * v * (1.0 - u) * P.r_tau_d -
-           p * v * (u - P.u_c) * P.r_tau_d - (1.0 - p) * P.r_tau_0;
+           P.k_fk * w * ds * P.r_2tau_si + p * v * (1.0 - u) * P.r_tau_d -
+           p * v * (u - P.u_c) * P.r_tau_d - sp.c * P.r_tau_0;
     J.a3 = p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
-    J.a5 = (ts + 1.0) * P.r_2tau_si;
+    J.a5 = (2.0 * ss.s) * P.r_2tau_si;
     J.a1 = -hk * v * P.r_tau_vp - hk * (1.0 - v) * rtvm +
-           (1.0 - p) * (1.0 - v) * (0.5 * dq * P.ksm * P.dv12) * (rtvm * rtvm);
-    J.a4 = -p * P.r_tau_vp - (1.0 - p) * rtvm;
+           sp.c * (1.0 - v) * (0.5 * dq * P.ksm * P.dv12) * (rtvm * rtvm);
+    J.a4 = -p * P.r_tau_vp - sp.c * rtvm;
     J.a2 = -hk * w * P.r_tau_wp - hk * (1.0 - w) * P.r_tau_wm;
-    J.a6 = -p * P.r_tau_wp - (1.0 - p) * P.r_tau_wm;
+    J.a6 = -p * P.r_tau_wp - sp.c * P.r_tau_wm;
     return J;
 }
 

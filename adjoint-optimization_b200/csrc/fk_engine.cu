@@ -239,7 +239,7 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
 
 int64_t Problem::device_bytes() const {
     const DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_,
-                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &y0res_};
+                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &y0res_, &stg_};
     int64_t s = 0;
     for (auto* b : all) s += (int64_t)b->bytes;
     return s;
@@ -481,6 +481,56 @@ fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
     return FKADJ_OK;
 }
 
+// Discrete-exact backward sweep: per step s (last to first) the forward step
+// from y_s is replayed once to store its stage states, then k_adj_exact maps
+// lambda_{s+1} -> lambda_s and leaves the three E-sensitivity partials.
+fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2) {
+    fkadj_status s;
+    const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
+    const int ntl = tiles_of(tile_, g_);
+    if (!stg_.p) {
+        CK(stg_.alloc(3 * state_bytes()), "alloc stage states");
+        CK(cudaMemsetAsync(stg_.p, 0xff, stg_.bytes, st_), "init stage states");
+    }
+    double* part = partial_.as<double>();
+    double* p1 = part;
+    double* p23 = part + (size_t)nt * ntl;
+    double* p4 = part + 2 * (size_t)nt * ntl;
+    double* scratch = state_buf(1);
+    double* stg = stg_.as<double>();
+    auto back = [&](int t, const double* y) -> fkadj_status {
+        CK(prof_begin(K_FWD), "profiling event");
+        CK(launch_fwd_step(tile_, P_, g_, y, scratch, gh_.as<double>(), Et_[t], Eh_[t], Et_[t + 1], st_, stg),
+           "stage replay");
+        CK(prof_end(K_FWD), "profiling event");
+        CK(prof_begin(K_ADJ), "profiling event");
+        CK(launch_adj_exact(tile_, P_, g_, lam, lam2, y, stg, wc_.as<uint8_t>(), gh_.as<double>(),
+                            p1 + (size_t)t * ntl, p23 + (size_t)t * ntl, p4 + (size_t)t * ntl, st_),
+           "exact adjoint step");
+        CK(prof_end(K_ADJ), "profiling event");
+        launches_ += 2;
+        std::swap(lam, lam2);
+        return FKADJ_OK;
+    };
+    if (tp.policy == FKADJ_CKPT_FULL) {
+        for (int t = nt - 1; t >= 0; --t)
+            if ((s = back(t, slot(t)))) return s;
+        return FKADJ_OK;
+    }
+    for (int k = K - 1; k >= 0; --k) {
+        const int s0 = k * c, s1 = std::min(s0 + c, nt);
+        auto st = [&](int t) -> double* {
+            if (t == s0) return slot(k);
+            return segslot(t - s0 - 1);
+        };
+        for (int t = s0; t < s1 - 1; ++t)
+            if ((s = step_forward(t, st(t), st(t + 1)))) return s;
+        for (int t = s1 - 1; t >= s0; --t)
+            if ((s = back(t, st(t)))) return s;
+    }
+    return FKADJ_OK;
+}
+
 fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, double* LE, double* Lcost,
                            double* gradE, double* yf) {
     fkadj_status s;
@@ -489,10 +539,11 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         set_error("gradE is null");
         return FKADJ_ERR_ARG;
     }
-    if (grad_mode_ != FKADJ_GRAD_REF) {
-        set_error("gradient mode not available");
+    if (grad_mode_ != FKADJ_GRAD_REF && grad_mode_ != FKADJ_GRAD_EXACT) {
+        set_error("unknown gradient mode");
         return FKADJ_ERR_ARG;
     }
+    const bool exact = grad_mode_ == FKADJ_GRAD_EXACT;
     if ((s = prepare_E(Et))) return s;
     TrajPlan tp;
     if ((s = plan_trajectory(tp))) return s;
@@ -503,10 +554,11 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         CK(yh_.alloc(state_bytes()), "alloc midpoint state");
         CK(cudaMemsetAsync(yh_.p, 0xff, yh_.bytes, st_), "init midpoint state");
     }
-    const size_t pbytes = (size_t)(nt_ + 1) * ntiles_ * sizeof(double);
+    const size_t prow = (size_t)(3 * nt_ + 1);  // exact mode keeps 3 rows per step
+    const size_t pbytes = prow * ntiles_ * sizeof(double);
     if (partial_.bytes < pbytes) {
         CK(partial_.alloc(pbytes), "alloc partials");
-        CK(zgh_.alloc((size_t)(nt_ + 1) * sizeof(double)), "alloc zgh");
+        CK(zgh_.alloc(prow * sizeof(double)), "alloc zgh");
     }
     const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
     const int ntl = tiles_of(tile_, g_);
@@ -530,10 +582,17 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     if ((s = run_objective(yT, &l0))) return s;
     double* z = zbuf_.as<double>();
     double* z2 = z + state_elems();
-    CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, z, st_), "scatter z");
     double* part = partial_.as<double>();
-    CK(launch_dot_gh(tile_, g_, z, gh_.as<double>(), part + (size_t)nt * ntl, st_), "z.gh");
-    launches_ += 2;
+    if (exact) {
+        // lambda(T) = dJ/dy(T) = -z(T); discrete adjoint sweep
+        CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), -1.0, z, st_), "scatter lambda");
+        ++launches_;
+        if ((s = grad_exact_backward(tp, z, z2))) return s;
+    } else {
+        CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, z, st_), "scatter z");
+        CK(launch_dot_gh(tile_, g_, z, gh_.as<double>(), part + (size_t)nt * ntl, st_), "z.gh");
+        launches_ += 2;
+    }
     // ---- backward sweep (cu-G:1866-1908)
     auto back_step = [&](int i, const double* ya, const double* yb) -> fkadj_status {
         CK(prof_begin(K_MID), "profiling event");
@@ -550,7 +609,9 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         std::swap(z, z2);
         return FKADJ_OK;
     };
-    if (tp.policy == FKADJ_CKPT_FULL) {
+    if (exact) {
+        // backward sweep done above
+    } else if (tp.policy == FKADJ_CKPT_FULL) {
         for (int i = nt; i > 0; --i)
             if ((s = back_step(i, slot(i - 1), slot(i)))) return s;
     } else {
@@ -567,10 +628,11 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
                 if ((s = back_step(i, st(i - 1), st(i)))) return s;
         }
     }
-    CK(launch_sum_rows(part, nt + 1, ntl, zgh_.as<double>(), st_), "reduce z.gh");
+    const int rows = exact ? 3 * nt : nt + 1;
+    CK(launch_sum_rows(part, rows, ntl, zgh_.as<double>(), st_), "reduce z.gh");
     ++launches_;
-    std::vector<double> zgh(nt + 1);
-    CK(cudaMemcpyAsync(zgh.data(), zgh_.p, (nt + 1) * sizeof(double), cudaMemcpyDeviceToHost, st_),
+    std::vector<double> zgh(rows);
+    CK(cudaMemcpyAsync(zgh.data(), zgh_.p, rows * sizeof(double), cudaMemcpyDeviceToHost, st_),
        "download z.gh");
     CK(cudaEventRecord(ev_[2], st_), "event");
     if (yf && (s = download_grid(yT, yf))) return s;
@@ -579,7 +641,20 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     double le = 0;
     for (int i = 0; i <= nt; ++i) le += Et_[i] * Et_[i];
     le *= dt_;
-    for (int i = 0; i <= nt; ++i) gradE[i] = alpha_ * Et_[i] - zgh[i];  // cu-G:1924-1926
+    if (exact) {
+        // rows: [0, nt) b.a1 -> sample s, [nt, 2nt) b.(a2+a3) -> half step s,
+        // [2nt, 3nt) b.a4 -> sample s+1; then the transposed spline maps the
+        // half-step sensitivities back onto the samples.
+        std::vector<double> gE(nt + 1, 0.0);
+        for (int t = 0; t < nt; ++t) {
+            gE[t] += zgh[t];
+            gE[t + 1] += zgh[2 * nt + t];
+        }
+        spline_->transpose_add(0.5, zgh.data() + nt, gE.data());
+        for (int i = 0; i <= nt; ++i) gradE[i] = (gE[i] + alpha_ * dt_ * Et_[i]) / dt_;
+    } else {
+        for (int i = 0; i <= nt; ++i) gradE[i] = alpha_ * Et_[i] - zgh[i];  // cu-G:1924-1926
+    }
     if (L0) *L0 = l0;
     if (LE) *LE = le;
     if (Lcost) *Lcost = 0.5 * l0 + 0.5 * alpha_ * le;

@@ -103,6 +103,7 @@ private:
     fkadj_status plan_trajectory(TrajPlan& tp);
     fkadj_status ensure_traj(const TrajPlan& tp);
     fkadj_status run_objective(const double* yT, double* L0);
+    fkadj_status grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2);
     fkadj_status download_grid(const double* d_state, double* host_dense);
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
     double* segslot(int k) const { return seg_.as<double>() + (size_t)k * state_elems(); }
@@ -128,6 +129,7 @@ private:
     DevBuf zgh_;       // nt+1
     DevBuf traj_, seg_;
     DevBuf y0res_;     // resident initial state
+    DevBuf stg_;       // stage states Y2, Y3, Y4 of one step (exact mode)
     bool have_y0_ = false;
     TrajPlan traj_plan_{};
 

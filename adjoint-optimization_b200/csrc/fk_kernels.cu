@@ -55,7 +55,7 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, double* __restrict_
                                           const double* __restrict__ Y0, double* __restrict__ D,
                                           const double* __restrict__ ghs, int ld, double Ev,
                                           double cY, double cD, double* __restrict__ out,
-                                          long long plane) {
+                                          long long plane, double* __restrict__ stage_out) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
     constexpr int IT = (N + NT - 1) / NT;
@@ -85,9 +85,12 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, double* __restrict_
                 out[plane + o] = (Y0[RN + s] + D[IN + d]) + cD * kv[it];
                 out[2 * plane + o] = (Y0[2 * RN + s] + D[2 * IN + d]) + cD * kw[it];
             } else {
-                Y[s] = Y0[s] + cY * ku[it];
-                Y[RN + s] = Y0[RN + s] + cY * kv[it];
-                Y[2 * RN + s] = Y0[2 * RN + s] + cY * kw[it];
+                const double nu = Y0[s] + cY * ku[it];
+                const double nv = Y0[RN + s] + cY * kv[it];
+                const double nw = Y0[2 * RN + s] + cY * kw[it];
+                Y[s] = nu;
+                Y[RN + s] = nv;
+                Y[2 * RN + s] = nw;
                 if (inner) {
                     if (MODE == 0) {
                         D[d] = cD * ku[it];
@@ -98,6 +101,12 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, double* __restrict_
                         D[IN + d] = D[IN + d] + cD * kv[it];
                         D[2 * IN + d] = D[2 * IN + d] + cD * kw[it];
                     }
+                    if (stage_out) {  // stage state kept for the discrete adjoint
+                        const long long o = (long long)r * ld + c;
+                        stage_out[o] = nu;
+                        stage_out[plane + o] = nv;
+                        stage_out[2 * plane + o] = nw;
+                    }
                 }
             }
         }
@@ -105,10 +114,13 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, double* __restrict_
     if (MODE != 2) __syncthreads();
 }
 
+// One RK4 step y -> y_out.  When `stages` is non-null the stage states
+// Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3 are stored there too
+// (three consecutive states), for the discrete-exact adjoint.
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin,
                                                  double* __restrict__ yout, const double* __restrict__ gh,
-                                                 double E0, double Eh, double E1) {
+                                                 double E0, double Eh, double E1, double* __restrict__ stages) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* Y = reinterpret_cast<double*>(smem_raw);
@@ -124,10 +136,14 @@ __global__ void __launch_bounds__(NT) k_fwd_step(DevModel P, DevGrid g, const do
     __syncthreads();
     const double* ghs = gh + off;
     const double dt = P.dt;
-    fwd_stage<3, TX, TY, NT, 0>(P, Y, Y0, D, ghs, g.ld, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, 0);
-    fwd_stage<2, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, 0);
-    fwd_stage<1, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, 0);
-    fwd_stage<0, TX, TY, NT, 2>(P, Y, Y0, D, ghs, g.ld, E1, 0.0, dt * 1.0 / 6.0, yout + off, g.plane);
+    const long long sst = 3 * g.plane;
+    double* s2 = stages ? stages + off : nullptr;
+    double* s3 = stages ? stages + sst + off : nullptr;
+    double* s4 = stages ? stages + 2 * sst + off : nullptr;
+    fwd_stage<3, TX, TY, NT, 0>(P, Y, Y0, D, ghs, g.ld, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, g.plane, s2);
+    fwd_stage<2, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, g.plane, s3);
+    fwd_stage<1, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, g.plane, s4);
+    fwd_stage<0, TX, TY, NT, 2>(P, Y, Y0, D, ghs, g.ld, E1, 0.0, dt * 1.0 / 6.0, yout + off, g.plane, nullptr);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -322,6 +338,130 @@ __global__ void __launch_bounds__(NT) k_adj_step(DevModel P, DevGrid g, const do
     if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
 
+// ------------------------------------------------------ exact-mode adjoint
+//
+// Discrete adjoint of one RK4 step y_{s+1} = y_s + dt/6 (k1 + 2k2 + 2k3 + k4):
+// with lambda = dJ/dy_{s+1} and g(a; Y) = L^T a + J_F(Y)^T a,
+//   a4 = dt/6 lam,                 mu4 = g(a4; Y4)
+//   a3 = dt/3 lam + dt   mu4,      mu3 = g(a3; Y3)
+//   a2 = dt/3 lam + dt/2 mu3,      mu2 = g(a2; Y2)
+//   a1 = dt/6 lam + dt/2 mu2,      mu1 = g(a1; y_s)
+//   lam_s = lam + (mu4 + mu3 + mu2 + mu1)
+// and the E sensitivities b.a1 (sample s), b.(a2 + a3) (half step s) and
+// b.a4 (sample s+1), b = gh on u.  Same temporal blocking as the reference
+// mode: a_s lives in shared memory on the tile grown by (4 - s) cells.
+template <int E, int TX, int TY, int NT, int MODE>
+__device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g, double* __restrict__ A,
+                                            const double* __restrict__ L0, double* __restrict__ D,
+                                            const uint8_t* __restrict__ wc, const double* __restrict__ ys,
+                                            long long off, double cL, double cM, double* __restrict__ out,
+                                            const double* __restrict__ ghs, double& acc) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
+    constexpr int IT = (N + NT - 1) / NT;
+    constexpr int IN = TX * TY;
+    double ku[IT], kv[IT], kw[IT];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = threadIdx.x + it * NT;
+        if (q < N) {
+            const int r = HALO - E + q / W, c = HALO - E + q % W;
+            const int s = r * RW + c;
+            const long long o = off + (long long)r * g.ld + c;
+            if (isnan(A[s])) {
+                ku[it] = kv[it] = kw[it] = A[s];
+            } else {
+                const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+                adj_at<RW, RN>(P, A, s, __ldg(wc + o), J, ku[it], kv[it], kw[it]);
+            }
+        }
+    }
+    if (MODE != 2) __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = threadIdx.x + it * NT;
+        if (q < N) {
+            const int r = HALO - E + q / W, c = HALO - E + q % W;
+            const int s = r * RW + c;
+            const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+            const int d = (r - HALO) * TX + (c - HALO);
+            if (MODE == 2) {
+                const long long o = (long long)r * g.ld + c;
+                out[o] = L0[s] + (D[d] + ku[it]);
+                out[g.plane + o] = L0[RN + s] + (D[IN + d] + kv[it]);
+                out[2 * g.plane + o] = L0[2 * RN + s] + (D[2 * IN + d] + kw[it]);
+            } else {
+                const double au = cL * L0[s] + cM * ku[it];
+                A[s] = au;
+                A[RN + s] = cL * L0[RN + s] + cM * kv[it];
+                A[2 * RN + s] = cL * L0[2 * RN + s] + cM * kw[it];
+                if (inner) {
+                    if (MODE == 0) {
+                        D[d] = ku[it];
+                        D[IN + d] = kv[it];
+                        D[2 * IN + d] = kw[it];
+                    } else {
+                        D[d] = D[d] + ku[it];
+                        D[IN + d] = D[IN + d] + kv[it];
+                        D[2 * IN + d] = D[2 * IN + d] + kw[it];
+                    }
+                    const double t = au * __ldg(ghs + (long long)r * g.ld + c);
+                    if (!isnan(t)) acc += t;
+                }
+            }
+        }
+    }
+    if (MODE != 2) __syncthreads();
+}
+
+// lam (state of lambda_{s+1}) -> lamout (lambda_s); y = y_s; stages = Y2, Y3,
+// Y4 of step s (three consecutive states, written by k_fwd_step).
+// Per tile: p1 <- b.a1, p23 <- b.(a2 + a3), p4 <- b.a4.
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_adj_exact(DevModel P, DevGrid g, const double* __restrict__ lam,
+                                                  double* __restrict__ lamout, const double* __restrict__ y,
+                                                  const double* __restrict__ stages,
+                                                  const uint8_t* __restrict__ wc, const double* __restrict__ gh,
+                                                  double* __restrict__ p1, double* __restrict__ p23,
+                                                  double* __restrict__ p4) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    constexpr int IN = TX * TY;
+    extern __shared__ double4 smem_raw[];
+    double* A = reinterpret_cast<double*>(smem_raw);
+    double* L0 = A + 3 * RN;
+    double* D = L0 + 3 * RN;
+    double* red = D + 3 * IN;
+    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const long long off = (long long)i0 * g.ld + j0;
+    const bool vec_ok = ((g.ld | j0) & 1) == 0;
+    load_region<RH, RW, NT>(L0, lam + off, g.ld, g.plane, vec_ok);
+    __syncthreads();
+    const double dt = P.dt;
+    const double c6 = dt / 6.0, c3 = dt / 3.0, c2 = dt * 0.5;
+    for (int q = threadIdx.x; q < 3 * RN; q += NT) A[q] = c6 * L0[q];
+    // b.a4 over the tile
+    const double* ghs = gh + off;
+    double acc4 = 0.0, acc23 = 0.0, acc1 = 0.0;
+    for (int q = threadIdx.x; q < IN; q += NT) {
+        const int r = HALO + q / TX, c = HALO + q % TX;
+        const double t = c6 * L0[r * RW + c] * __ldg(ghs + (long long)r * g.ld + c);
+        if (!isnan(t)) acc4 += t;
+    }
+    __syncthreads();
+    const long long sst = 3 * g.plane;
+    exact_stage<3, TX, TY, NT, 0>(P, g, A, L0, D, wc, stages + 2 * sst, off, c3, dt, nullptr, ghs, acc23);
+    exact_stage<2, TX, TY, NT, 1>(P, g, A, L0, D, wc, stages + sst, off, c3, c2, nullptr, ghs, acc23);
+    exact_stage<1, TX, TY, NT, 1>(P, g, A, L0, D, wc, stages, off, c6, c2, nullptr, ghs, acc1);
+    exact_stage<0, TX, TY, NT, 2>(P, g, A, L0, D, wc, y, off, 0.0, 0.0, lamout + off, ghs, acc1);
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    double s = block_sum<NT>(acc1, red);
+    if (threadIdx.x == 0) p1[tile] = s;
+    s = block_sum<NT>(acc23, red);
+    if (threadIdx.x == 0) p23[tile] = s;
+    s = block_sum<NT>(acc4, red);
+    if (threadIdx.x == 0) p4[tile] = s;
+}
+
 // z_u . gh over one tile (NaN terms skipped) -> partial[tile].
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) k_dot_gh(DevGrid g, const double* __restrict__ z,
@@ -428,6 +568,8 @@ static cudaError_t setup_tile() {
     if (e) return e;
     e = cudaFuncSetAttribute(k_adj_mid<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid_smem<TX, TY, NT>());
     if (e) return e;
+    e = cudaFuncSetAttribute(k_adj_exact<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem<TX, TY, NT>());
+    if (e) return e;
     return cudaFuncSetAttribute(k_adj_step<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem<TX, TY, NT>());
 }
 
@@ -465,9 +607,18 @@ static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
 }
 
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
-                            const double* gh, double E0, double Eh, double E1, cudaStream_t st) {
+                            const double* gh, double E0, double Eh, double E1, cudaStream_t st,
+                            double* stages) {
     DISPATCH(tile, (k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, fwd_smem<TX, TY, NT>(), st>>>(
-                        P, g, yin, yout, gh, E0, Eh, E1)));
+                        P, g, yin, yout, gh, E0, Eh, E1, stages)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, const double* lam, double* lamout,
+                             const double* y, const double* stages, const uint8_t* wc, const double* gh,
+                             double* p1, double* p23, double* p4, cudaStream_t st) {
+    DISPATCH(tile, (k_adj_exact<TX, TY, NT><<<tile_grid(g, TX, TY), NT, adj_smem<TX, TY, NT>(), st>>>(
+                        P, g, lam, lamout, y, stages, wc, gh, p1, p23, p4)));
     return cudaGetLastError();
 }
 

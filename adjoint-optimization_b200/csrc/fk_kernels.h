@@ -25,7 +25,11 @@ int tiles_of(int tile, const DevGrid& g);
 cudaError_t kernels_init();
 
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
-                            const double* gh, double E0, double Eh, double E1, cudaStream_t st);
+                            const double* gh, double E0, double Eh, double E1, cudaStream_t st,
+                            double* stages = nullptr);
+cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, const double* lam, double* lamout,
+                             const double* y, const double* stages, const uint8_t* wc, const double* gh,
+                             double* p1, double* p23, double* p4, cudaStream_t st);
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
                            cudaStream_t st);

@@ -81,3 +81,31 @@ def test_compute_ns_matches_gateway_rule():
     assert compute_ns(2000, 100) == 19
     assert compute_ns(2000, 300) == 6
     assert compute_ns(10, 10) == 0
+
+
+def test_mex_compat_shim_compiles_and_links(tmp_path):
+    """The drop-in shim (reference names and signatures) compiles against a
+    MEX-API stand-in and links against libfkadj; the call with a bad grid
+    returns the status instead of exiting (no device work)."""
+    from fkadj import _lib
+    src = tmp_path / "gw.cpp"
+    src.write_text(r'''
+#include "matrix.h"
+#include "fkadj_mex_compat.h"
+#include <cstdio>
+int main() {
+    double Et[4] = {0, 0, 0, 0}, y0[3] = {0, 0, 0}, gh[1] = {0}, ys[3], yf[3];
+    int ai[1] = {1};
+    char *ps = nullptr;
+    int rc = fk_forward_Et_comp(0.1, Et, 3, y0, ai, 1, 1, 1, gh, 1, 0, ys, yf, &ps);
+    std::printf("rc=%d str=%d\n", rc, ps != nullptr && std::strstr(ps, "h = 0.035") != nullptr);
+    return rc == 1 ? 0 : 1;
+}
+''')
+    exe = tmp_path / "gw"
+    inc = [f"-I{os.path.join(ROOT, 'include')}", f"-I{os.path.join(ROOT, 'oracle', 'ref_shim')}"]
+    subprocess.run(["g++", "-std=c++17", *inc, str(src), "-o", str(exe), _lib.LIB_PATH,
+                    f"-Wl,-rpath,{os.path.dirname(_lib.LIB_PATH)}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "rc=1 str=1" in out.stdout

@@ -105,3 +105,48 @@ def test_problem_handle_repeated_calls_are_deterministic():
         assert pb.device_bytes > 0
     assert np.array_equal(a["gradE"], b["gradE"])
     assert a["Lcost"] == b["Lcost"] == o["Lcost"]
+
+
+def _exact(inst, alpha=0.2, ckpt=_lib.CKPT_AUTO, Et=None):
+    Et = inst.Et if Et is None else Et
+    return api.fk_grad_Et(Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                          inst.ghost, inst.gamma, inst.S, alpha, params=inst.params,
+                          opts=api.options(grad_mode=_lib.GRAD_EXACT, ckpt_policy=ckpt))
+
+
+@pytest.mark.parametrize("objective", ["mean_u2", "gradient"])
+def test_exact_gradient_matches_oracle(objective):
+    inst = _inst(48, 90, seed=31, objective=objective, ncols=64)
+    g, Lc, L0, LE, _ = _exact(inst)
+    r = O.grad(inst.params, inst.dt, inst.Et, inst.nt, inst.nrows, inst.ncols, inst.y0_grid, inst.gh_grid,
+               inst.active_index, O.Objective(inst.S, inst.gamma), 0.2, mode="exact")
+    assert abs(Lc - r["Lcost"]) <= 1e-10 * abs(r["Lcost"])
+    assert np.linalg.norm(g - r["gradE"]) <= 1e-8 * np.linalg.norm(r["gradE"])
+
+
+def test_exact_sqrt_equals_full():
+    inst = _inst(64, 130, seed=9)
+    a = _exact(inst, ckpt=_lib.CKPT_FULL)
+    b = _exact(inst, ckpt=_lib.CKPT_SQRT)
+    assert np.array_equal(a[0], b[0])
+
+
+def test_exact_gradient_central_fd_on_intervals():
+    """dJ/dA_k for piecewise-constant amplitudes (central FD, h = 1e-6) on
+    10 seeded intervals vs the discrete adjoint: dJ/dA_k = dt * sum_{i in k} gradE[i]."""
+    inst = W.make_instance(64, 400, seed=41, n_obstacles=8, intervals=40, wavefronts=4)
+    alpha = 0.0
+    g = _exact(inst, alpha)[0]
+    K = len(inst.amplitudes)
+    dJdA = np.array([inst.dt * g[inst.interval_of_sample == k].sum() for k in range(K)])
+    rng = np.random.default_rng(2024)
+    h = 1e-6
+    with api.Problem(inst, opts=api.options(grad_mode=_lib.GRAD_EXACT)) as pb:
+        for k in rng.choice(K, size=10, replace=False):
+            Ap, Am = inst.amplitudes.copy(), inst.amplitudes.copy()
+            Ap[k] += h
+            Am[k] -= h
+            Jp = pb.objective(W.piecewise_constant(inst.nt, Ap)[0], inst.y0)["Lcost"]
+            Jm = pb.objective(W.piecewise_constant(inst.nt, Am)[0], inst.y0)["Lcost"]
+            fd = (Jp - Jm) / (2 * h)
+            assert abs(fd - dJdA[k]) <= 1e-6 * np.abs(dJdA).max() + 1e-5 * abs(fd), (k, fd, dJdA[k])
