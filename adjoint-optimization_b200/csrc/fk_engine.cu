@@ -162,9 +162,12 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     g_.plane = (long long)g_.rows_alloc * g_.ld;
     P_ = make_model(p, dt);
     hw_ = make_hermite();
-    tile_ = (o.tile > 0 && o.tile < tile_count()) ? o.tile : 0;
-    ntiles_ = 0;
-    for (int t = 0; t < tile_count(); ++t) ntiles_ = std::max(ntiles_, tiles_of(t, g_));
+    // options.tile: 0 = autotune at first use, k >= 1 = preset k-1 for every kernel
+    autotune_ = o.tile <= 0 || o.tile > tile_count();
+    for (int& t : tk_) t = autotune_ ? 0 : o.tile - 1;
+    tuned_ = !autotune_;
+    subblock_lattice(g_, &nsbx_, &nsby_);
+    nsb_ = nsbx_ * nsby_;
 
     // geometry on the padded grid: gh, adjoint stencil weights, compact positions
     const size_t pl = (size_t)g_.plane;
@@ -328,7 +331,7 @@ void Problem::kernel_time(int k, double* avg_ms, int64_t* samples) const {
 
 fkadj_status Problem::step_forward(int i, const double* yin, double* yout) {
     CK(prof_begin(K_FWD), "profiling event");
-    CK(launch_fwd_step(tile_, P_, g_, yin, yout, gh_.as<double>(), Et_[i], Eh_[i], Et_[i + 1], st_),
+    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), Et_[i], Eh_[i], Et_[i + 1], st_),
        "forward step");
     CK(prof_end(K_FWD), "profiling event");
     ++launches_;
@@ -358,6 +361,10 @@ fkadj_status Problem::forward(const double* Et, const double* y_ini, int nstep, 
     CK(cudaEventRecord(ev_[0], st_), "event");
     double* b0 = state_buf(0);
     if ((s = upload_state(y_ini, b0))) return s;
+    if (autotune_ && !tuned_fwd_) {
+        if ((s = autotune())) return s;
+        tuned_fwd_ = true;
+    }
     double* cur = b0;
     const size_t n3 = (size_t)3 * g_.nrows * g_.ncols;
     for (int i = 0; i < nt_; ++i) {
@@ -410,6 +417,10 @@ fkadj_status Problem::objective(const double* Et, const double* y_ini, double* L
     CK(cudaEventRecord(ev_[0], st_), "event");
     double* cur = state_buf(0);
     if ((s = upload_state(y_ini, cur))) return s;
+    if (autotune_ && !tuned_fwd_) {
+        if ((s = autotune())) return s;
+        tuned_fwd_ = true;
+    }
     for (int i = 0; i < nt_; ++i) {
         double* out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
         if ((s = step_forward(i, cur, out))) return s;
@@ -481,31 +492,111 @@ fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
     return FKADJ_OK;
 }
 
+fkadj_status Problem::ensure_adjoint_work() {
+    if (!zbuf_.p) {
+        CK(zbuf_.alloc(2 * state_bytes()), "alloc adjoint states");
+        CK(cudaMemsetAsync(zbuf_.p, 0xff, zbuf_.bytes, st_), "init adjoint states");
+    }
+    if (grad_mode_ == FKADJ_GRAD_REF && !yh_.p) {
+        CK(yh_.alloc(state_bytes()), "alloc midpoint state");
+        CK(cudaMemsetAsync(yh_.p, 0xff, yh_.bytes, st_), "init midpoint state");
+    }
+    if (grad_mode_ == FKADJ_GRAD_EXACT && !stg_.p) {
+        CK(stg_.alloc(3 * state_bytes()), "alloc stage states");
+        CK(cudaMemsetAsync(stg_.p, 0xff, stg_.bytes, st_), "init stage states");
+    }
+    const size_t prow = (size_t)(3 * nt_ + 1);  // exact mode keeps 3 rows per step
+    const size_t pbytes = prow * (size_t)nsb_ * sizeof(double);
+    if (partial_.bytes < pbytes) {
+        CK(partial_.alloc(pbytes), "alloc partials");
+        CK(cudaMemsetAsync(partial_.p, 0, partial_.bytes, st_), "zero partials");
+        CK(zgh_.alloc(prow * sizeof(double)), "alloc zgh");
+    }
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::autotune() {
+    const double* y = y0res_.as<double>();
+    double* out = state_buf(1);
+    cudaEvent_t a = nullptr, b = nullptr;
+    CK(cudaEventCreate(&a), "event");
+    CK(cudaEventCreate(&b), "event");
+    const double E = Et_.empty() ? 0.0 : Et_[0];
+    auto timed = [&](auto&& launch, float* ms) -> cudaError_t {
+        cudaError_t e = launch();
+        if (e) return e;
+        if ((e = cudaEventRecord(a, st_))) return e;
+        for (int r = 0; r < 3; ++r)
+            if ((e = launch())) return e;
+        if ((e = cudaEventRecord(b, st_))) return e;
+        if ((e = cudaEventSynchronize(b))) return e;
+        return cudaEventElapsedTime(ms, a, b);
+    };
+    auto pick = [&](int kind, auto&& make_launch) -> cudaError_t {
+        float best = 1e30f;
+        for (int t = 0; t < tile_count(); ++t) {
+            float ms = 0;
+            cudaError_t e = timed([&]() { return make_launch(t); }, &ms);
+            if (e) return e;
+            launches_ += 4;
+            if (ms < best) best = ms, tk_[kind] = t;
+        }
+        return cudaSuccess;
+    };
+    cudaError_t e = pick(T_FWD, [&](int t) {
+        return launch_fwd_step(t, P_, g_, y, out, gh_.as<double>(), E, E, E, st_);
+    });
+    if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_REF) {
+        double* z2 = zbuf_.as<double>() + state_elems();
+        e = pick(T_MID, [&](int t) {
+            return launch_adj_mid(t, P_, g_, y, y, gh_.as<double>(), yh_.as<double>(), E, E, E, hw_, st_);
+        });
+        if (!e)
+            e = pick(T_ADJ, [&](int t) {
+                return launch_adj_step(t, P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
+                                       partial_.as<double>(), nsbx_, st_);
+            });
+    }
+    if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_EXACT) {
+        double* z2 = zbuf_.as<double>() + state_elems();
+        e = launch_fwd_step(tk_[T_FWD], P_, g_, y, out, gh_.as<double>(), E, E, E, st_, stg_.as<double>());
+        if (!e)
+            e = pick(T_EXACT, [&](int t) {
+                double* p = partial_.as<double>();
+                return launch_adj_exact(t, P_, g_, y, z2, y, stg_.as<double>(), wc_.as<uint8_t>(),
+                                        gh_.as<double>(), p, p + nsb_, p + 2 * (size_t)nsb_, nsbx_, st_);
+            });
+    }
+    // the trial launches wrote scratch partials: clear them
+    if (!e && partial_.p) e = cudaMemsetAsync(partial_.p, 0, partial_.bytes, st_);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(e, "autotune");
+    return FKADJ_OK;
+}
+
 // Discrete-exact backward sweep: per step s (last to first) the forward step
 // from y_s is replayed once to store its stage states, then k_adj_exact maps
 // lambda_{s+1} -> lambda_s and leaves the three E-sensitivity partials.
 fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2) {
     fkadj_status s;
     const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
-    const int ntl = tiles_of(tile_, g_);
-    if (!stg_.p) {
-        CK(stg_.alloc(3 * state_bytes()), "alloc stage states");
-        CK(cudaMemsetAsync(stg_.p, 0xff, stg_.bytes, st_), "init stage states");
-    }
+    const size_t nsb = (size_t)nsb_;
     double* part = partial_.as<double>();
     double* p1 = part;
-    double* p23 = part + (size_t)nt * ntl;
-    double* p4 = part + 2 * (size_t)nt * ntl;
+    double* p23 = part + (size_t)nt * nsb;
+    double* p4 = part + 2 * (size_t)nt * nsb;
     double* scratch = state_buf(1);
     double* stg = stg_.as<double>();
     auto back = [&](int t, const double* y) -> fkadj_status {
         CK(prof_begin(K_FWD), "profiling event");
-        CK(launch_fwd_step(tile_, P_, g_, y, scratch, gh_.as<double>(), Et_[t], Eh_[t], Et_[t + 1], st_, stg),
+        CK(launch_fwd_step(tk_[T_FWD], P_, g_, y, scratch, gh_.as<double>(), Et_[t], Eh_[t], Et_[t + 1], st_,
+                           stg),
            "stage replay");
         CK(prof_end(K_FWD), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
-        CK(launch_adj_exact(tile_, P_, g_, lam, lam2, y, stg, wc_.as<uint8_t>(), gh_.as<double>(),
-                            p1 + (size_t)t * ntl, p23 + (size_t)t * ntl, p4 + (size_t)t * ntl, st_),
+        CK(launch_adj_exact(tk_[T_EXACT], P_, g_, lam, lam2, y, stg, wc_.as<uint8_t>(), gh_.as<double>(),
+                            p1 + t * nsb, p23 + t * nsb, p4 + t * nsb, nsbx_, st_),
            "exact adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
@@ -548,23 +639,16 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     TrajPlan tp;
     if ((s = plan_trajectory(tp))) return s;
     if ((s = ensure_traj(tp))) return s;
-    if (!zbuf_.p) {
-        CK(zbuf_.alloc(2 * state_bytes()), "alloc adjoint states");
-        CK(cudaMemsetAsync(zbuf_.p, 0xff, zbuf_.bytes, st_), "init adjoint states");
-        CK(yh_.alloc(state_bytes()), "alloc midpoint state");
-        CK(cudaMemsetAsync(yh_.p, 0xff, yh_.bytes, st_), "init midpoint state");
-    }
-    const size_t prow = (size_t)(3 * nt_ + 1);  // exact mode keeps 3 rows per step
-    const size_t pbytes = prow * ntiles_ * sizeof(double);
-    if (partial_.bytes < pbytes) {
-        CK(partial_.alloc(pbytes), "alloc partials");
-        CK(zgh_.alloc(prow * sizeof(double)), "alloc zgh");
-    }
+    if ((s = ensure_adjoint_work())) return s;
     const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
-    const int ntl = tiles_of(tile_, g_);
+    const size_t nsb = (size_t)nsb_;
     CK(cudaEventRecord(ev_[0], st_), "event");
     // ---- forward sweep, storing states (cu-G:1689-1724 without the D2H copies)
     if ((s = upload_state(y_ini, slot(0)))) return s;
+    if (autotune_ && !tuned_) {
+        if ((s = autotune())) return s;
+        tuned_ = tuned_fwd_ = true;
+    }
     double* cur = slot(0);
     for (int i = 0; i < nt; ++i) {
         double* out;
@@ -590,19 +674,19 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         if ((s = grad_exact_backward(tp, z, z2))) return s;
     } else {
         CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, z, st_), "scatter z");
-        CK(launch_dot_gh(tile_, g_, z, gh_.as<double>(), part + (size_t)nt * ntl, st_), "z.gh");
+        CK(launch_dot_gh(g_, z, gh_.as<double>(), part + (size_t)nt * nsb, nsbx_, nsby_, st_), "z.gh");
         launches_ += 2;
     }
     // ---- backward sweep (cu-G:1866-1908)
     auto back_step = [&](int i, const double* ya, const double* yb) -> fkadj_status {
         CK(prof_begin(K_MID), "profiling event");
-        CK(launch_adj_mid(tile_, P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), Et_[i - 1], Et_[i],
+        CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), Et_[i - 1], Et_[i],
                           E3_[i - 1], hw_, st_),
            "adjoint midpoint");
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
-        CK(launch_adj_step(tile_, P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(), gh_.as<double>(),
-                           part + (size_t)(i - 1) * ntl, st_),
+        CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
+                           gh_.as<double>(), part + (size_t)(i - 1) * nsb, nsbx_, st_),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
@@ -629,7 +713,7 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         }
     }
     const int rows = exact ? 3 * nt : nt + 1;
-    CK(launch_sum_rows(part, rows, ntl, zgh_.as<double>(), st_), "reduce z.gh");
+    CK(launch_sum_rows(part, rows, nsb_, zgh_.as<double>(), st_), "reduce z.gh");
     ++launches_;
     std::vector<double> zgh(rows);
     CK(cudaMemcpyAsync(zgh.data(), zgh_.p, rows * sizeof(double), cudaMemcpyDeviceToHost, st_),

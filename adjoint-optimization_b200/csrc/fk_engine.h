@@ -81,8 +81,14 @@ public:
     int nt() const { return nt_; }
     int n_num() const { return n_num_; }
     cudaStream_t stream() const { return st_; }
-    int tile() const { return tile_; }
-    void set_tile(int t) { tile_ = t; }
+    // tile preset per kernel kind; chosen by autotune() unless fixed by options
+    enum TileKind { T_FWD = 0, T_MID = 1, T_ADJ = 2, T_EXACT = 3 };
+    int tile(int kind) const { return tk_[kind]; }
+    void set_tile(int kind, int t) { tk_[kind] = t; }
+    // Times every tile preset of every kernel kind on the current initial
+    // state (a few launches each) and keeps the fastest per kind.  Results do
+    // not depend on the choice (fixed-order reductions).
+    fkadj_status autotune();
 
     // Lower-level pieces (used by the batch / serving layers and the tests).
     // upload_state with y_ini == nullptr re-uses the initial state of the
@@ -104,6 +110,7 @@ private:
     fkadj_status ensure_traj(const TrajPlan& tp);
     fkadj_status run_objective(const double* yT, double* L0);
     fkadj_status grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2);
+    fkadj_status ensure_adjoint_work();
     fkadj_status download_grid(const double* d_state, double* host_dense);
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
     double* segslot(int k) const { return seg_.as<double>() + (size_t)k * state_elems(); }
@@ -113,7 +120,9 @@ private:
     DevGrid g_{};
     HermiteW hw_{};
     double dt_ = 0, alpha_ = 0, gamma_[3] = {0, 0, 0};
-    int nt_ = 0, n_num_ = 0, tile_ = 0, device_ = 0, ntiles_ = 0;
+    int nt_ = 0, n_num_ = 0, device_ = 0, nsbx_ = 0, nsby_ = 0, nsb_ = 0;
+    int tk_[4] = {0, 0, 0, 0};  // tile preset per kernel kind (TileKind)
+    bool autotune_ = true, tuned_ = false, tuned_fwd_ = false;
     bool own_stream_ = false, have_obj_ = false;
     int grad_mode_ = FKADJ_GRAD_REF, ckpt_policy_ = FKADJ_CKPT_AUTO;
     int64_t ckpt_budget_ = 0;

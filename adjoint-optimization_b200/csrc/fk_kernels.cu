@@ -7,8 +7,15 @@
 // stage needs another CTA's data (temporal blocking over the RK stages).
 // Global traffic per cell and step is therefore one read and one write of the
 // state plus gh (56 B), instead of the reference's four launches and ~440 B
-// (cu-F:766-793).  The work is FP64 arithmetic (3 tanh per vector-field
-// evaluation), so the tile shape trades halo recompute against occupancy.
+// (cu-F:766-793).
+//
+// The work is FP64 arithmetic (three exp-based smoothed steps and one division
+// per vector-field evaluation), so the kernels are written for issue
+// efficiency: stage inputs ping-pong between two shared buffers (no per-thread
+// register arrays across barriers, loops stay rolled and the code fits the
+// instruction cache), the step-start state is re-read from L1/L2 instead of
+// occupying shared memory, and the interior accumulator is the only other
+// shared buffer.
 #include "fk_kernels.h"
 
 #include <cstdio>
@@ -17,15 +24,23 @@ namespace fkadj {
 
 namespace {
 
-// Copies a rows x width window of the three planes at src (row pitch ld, plane
-// pitch plane) into shared memory (row pitch width, plane pitch rn), with
-// 16-byte vector loads when the window is 16-byte aligned.
+constexpr double kNaN = __builtin_nan("");
+
+// Resident CTAs per SM the register allocation targets: what shared memory
+// allows for the tile (101 KB at 32x32, 58 KB at 32x16 and below, one
+// 512-thread CTA).
+constexpr int min_blocks(int tx, int ty, int nt) { return nt >= 512 ? 1 : (tx * ty <= 512 ? 3 : 2); }
+
+// Copies a ROWS x WIDTH window of the three planes at src (row pitch ld, plane
+// pitch plane) into shared memory (row pitch WIDTH, plane pitch ROWS*WIDTH),
+// with 16-byte vector loads when the window is 16-byte aligned.
 template <int ROWS, int WIDTH, int NT>
 __device__ __forceinline__ void load_region(double* __restrict__ dst, const double* __restrict__ src,
                                             int ld, long long plane, bool vec_ok) {
     constexpr int RN = ROWS * WIDTH;
     if (vec_ok && (WIDTH % 2) == 0) {
         constexpr int HW = WIDTH / 2;
+#pragma unroll 2
         for (int q = threadIdx.x; q < 3 * ROWS * HW; q += NT) {
             const int f = q / (ROWS * HW);
             const int rem = q - f * (ROWS * HW);
@@ -34,6 +49,7 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
             reinterpret_cast<double2*>(dst + f * RN + r * WIDTH)[c2] = v;
         }
     } else {
+#pragma unroll 2
         for (int q = threadIdx.x; q < 3 * RN; q += NT) {
             const int f = q / RN;
             const int rem = q - f * RN;
@@ -43,70 +59,97 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
     }
 }
 
+// Fixed-order block sum (warp shuffles, then warps in order); result valid in
+// thread 0.  All threads of the block must call it.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int w = 0; w < NT / 32; ++w) s += red[w];
+    }
+    return s;
+}
+
+// Sums of a per-cell term over the 16x16 sub-blocks of a tile, in an order
+// fixed by the sub-block alone (lane l adds the 8 cells of half-row l in
+// column order, then a shuffle tree): the result does not depend on the tile
+// preset or the thread count, so gradients are bit-identical whichever tile
+// the autotuner picks.  term(r, c) takes interior coordinates and returns 0
+// for cells that contribute nothing.  One partial per sub-block goes to
+// row[sub-block index on the grid's 16x16 lattice].
+template <int TX, int TY, int NT, class Term>
+__device__ __forceinline__ void subblock_sums(Term term, double* __restrict__ row, int i0, int j0, int nsbx) {
+    constexpr int SBX = TX / 16, SBY = TY / 16, NSB = SBX * SBY, NW = NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int b = w; b < NSB; b += NW) {
+        const int by = b / SBX, bx = b - by * SBX;
+        const int r = by * 16 + (lane >> 1), c0 = bx * 16 + (lane & 1) * 8;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += term(r, c0 + k);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) row[(long long)(i0 / 16 + by) * nsbx + (j0 / 16 + bx)] = s;
+    }
+}
+
 // ---------------------------------------------------------------- forward
 
-// One forward RK stage evaluated on the tile grown by E cells.
-//   MODE 0: first stage   Y <- Y0 + cY*k, D  = cD*k
-//   MODE 1: middle stage  Y <- Y0 + cY*k, D += cD*k
-//   MODE 2: last stage    out <- (Y0 + D) + cD*k   (interior only)
-// Stage algebra and E sources of cu-F:459-562 / cu-F:766-793.
+// One forward RK stage on the tile grown by E cells: k = f(src), then
+//   MODE 0: dst = y0 + cY*k, D  = cD*k        (first stage)
+//   MODE 1: dst = y0 + cY*k, D += cD*k        (middle stages)
+//   MODE 2: out = (y0 + D) + cD*k             (last stage, interior only)
+// y0 (the step-start state) comes from global memory; stage algebra and E
+// sources of cu-F:459-562 / cu-F:766-793.
 template <int E, int TX, int TY, int NT, int MODE>
-__device__ __forceinline__ void fwd_stage(const DevModel& P, double* __restrict__ Y,
-                                          const double* __restrict__ Y0, double* __restrict__ D,
-                                          const double* __restrict__ ghs, int ld, double Ev,
-                                          double cY, double cD, double* __restrict__ out,
-                                          long long plane, double* __restrict__ stage_out) {
+__device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __restrict__ src,
+                                          double* __restrict__ dst, double* __restrict__ D,
+                                          const double* __restrict__ y0g, const double* __restrict__ ghs,
+                                          int ld, long long plane, double Ev, double cY, double cD,
+                                          double* __restrict__ out, double* __restrict__ stage_out) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
-    constexpr int IT = (N + NT - 1) / NT;
     constexpr int IN = TX * TY;
-    double ku[IT], kv[IT], kw[IT];
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int q = threadIdx.x + it * NT;
-        if (q < N) {
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
-            const double g = __ldg(ghs + (long long)r * ld + c);
-            rhs_at<RW, RN>(P, Y, r * RW + c, Ev * g, ku[it], kv[it], kw[it]);
-        }
-    }
-    if (MODE != 2) __syncthreads();
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int q = threadIdx.x + it * NT;
-        if (q < N) {
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
-            const int s = r * RW + c;
-            const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
-            const int d = (r - HALO) * TX + (c - HALO);
-            if (MODE == 2) {
-                const long long o = (long long)r * ld + c;
-                out[o] = (Y0[s] + D[d]) + cD * ku[it];
-                out[plane + o] = (Y0[RN + s] + D[IN + d]) + cD * kv[it];
-                out[2 * plane + o] = (Y0[2 * RN + s] + D[2 * IN + d]) + cD * kw[it];
-            } else {
-                const double nu = Y0[s] + cY * ku[it];
-                const double nv = Y0[RN + s] + cY * kv[it];
-                const double nw = Y0[2 * RN + s] + cY * kw[it];
-                Y[s] = nu;
-                Y[RN + s] = nv;
-                Y[2 * RN + s] = nw;
-                if (inner) {
-                    if (MODE == 0) {
-                        D[d] = cD * ku[it];
-                        D[IN + d] = cD * kv[it];
-                        D[2 * IN + d] = cD * kw[it];
-                    } else {
-                        D[d] = D[d] + cD * ku[it];
-                        D[IN + d] = D[IN + d] + cD * kv[it];
-                        D[2 * IN + d] = D[2 * IN + d] + cD * kw[it];
-                    }
-                    if (stage_out) {  // stage state kept for the discrete adjoint
-                        const long long o = (long long)r * ld + c;
-                        stage_out[o] = nu;
-                        stage_out[plane + o] = nv;
-                        stage_out[2 * plane + o] = nw;
-                    }
+#pragma unroll 1
+    for (int q = threadIdx.x; q < N; q += NT) {
+        const int r = HALO - E + q / W, c = HALO - E + q % W;
+        const int s = r * RW + c;
+        const long long o = (long long)r * ld + c;
+        double ku, kv, kw;
+        rhs_at<RW, RN>(P, src, s, Ev * __ldg(ghs + o), ku, kv, kw);
+        const double a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
+        const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+        const int d = (r - HALO) * TX + (c - HALO);
+        if (MODE == 2) {
+            out[o] = (a + D[d]) + cD * ku;
+            out[plane + o] = (b + D[IN + d]) + cD * kv;
+            out[2 * plane + o] = (e + D[2 * IN + d]) + cD * kw;
+        } else {
+            const double nu = a + cY * ku, nv = b + cY * kv, nw = e + cY * kw;
+            dst[s] = nu;
+            dst[RN + s] = nv;
+            dst[2 * RN + s] = nw;
+            if (inner) {
+                if (MODE == 0) {
+                    D[d] = cD * ku;
+                    D[IN + d] = cD * kv;
+                    D[2 * IN + d] = cD * kw;
+                } else {
+                    D[d] = D[d] + cD * ku;
+                    D[IN + d] = D[IN + d] + cD * kv;
+                    D[2 * IN + d] = D[2 * IN + d] + cD * kw;
+                }
+                if (stage_out) {  // stage state kept for the discrete adjoint
+                    stage_out[o] = nu;
+                    stage_out[plane + o] = nv;
+                    stage_out[2 * plane + o] = nw;
                 }
             }
         }
@@ -118,32 +161,31 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, double* __restrict_
 // Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3 are stored there too
 // (three consecutive states), for the discrete-exact adjoint.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin,
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin,
                                                  double* __restrict__ yout, const double* __restrict__ gh,
                                                  double E0, double Eh, double E1, double* __restrict__ stages) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
-    double* Y = reinterpret_cast<double*>(smem_raw);
-    double* Y0 = Y + 3 * RN;
-    double* D = Y0 + 3 * RN;
+    double* A = reinterpret_cast<double*>(smem_raw);
+    double* B = A + 3 * RN;
+    double* D = B + 3 * RN;
     const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
     // region origin: logical (i0 - HALO, j0 - HALO) = padded (i0, j0)
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(Y, yin + off, g.ld, g.plane, vec_ok);
+    load_region<RH, RW, NT>(A, yin + off, g.ld, g.plane, vec_ok);
     __syncthreads();
-    for (int q = threadIdx.x; q < 3 * RN; q += NT) Y0[q] = Y[q];
-    __syncthreads();
+    const double* y0g = yin + off;
     const double* ghs = gh + off;
     const double dt = P.dt;
     const long long sst = 3 * g.plane;
     double* s2 = stages ? stages + off : nullptr;
     double* s3 = stages ? stages + sst + off : nullptr;
     double* s4 = stages ? stages + 2 * sst + off : nullptr;
-    fwd_stage<3, TX, TY, NT, 0>(P, Y, Y0, D, ghs, g.ld, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, g.plane, s2);
-    fwd_stage<2, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, g.plane, s3);
-    fwd_stage<1, TX, TY, NT, 1>(P, Y, Y0, D, ghs, g.ld, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, g.plane, s4);
-    fwd_stage<0, TX, TY, NT, 2>(P, Y, Y0, D, ghs, g.ld, E1, 0.0, dt * 1.0 / 6.0, yout + off, g.plane, nullptr);
+    fwd_stage<3, TX, TY, NT, 0>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2);
+    fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3);
+    fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4);
+    fwd_stage<0, TX, TY, NT, 2>(P, B, A, D, y0g, ghs, g.ld, g.plane, E1, 0.0, dt * 1.0 / 6.0, yout + off, nullptr);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -153,7 +195,7 @@ __global__ void __launch_bounds__(NT) k_fwd_step(DevModel P, DevGrid g, const do
 // (27/64) dt f(y3, E(t_{i-1}+dt/3)).  Halo 2: f(ya), f(yb) on the tile grown by
 // one cell, f(y3) on the tile.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya,
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya,
                                                 const double* __restrict__ yb,
                                                 const double* __restrict__ gh, double* __restrict__ yh,
                                                 double Ea, double Eb, double E3, HermiteW hw) {
@@ -172,134 +214,98 @@ __global__ void __launch_bounds__(NT) k_adj_mid(DevModel P, DevGrid g, const dou
     __syncthreads();
     const double dt = P.dt;
     {
-        constexpr int W = TX + 2, N = W * (TY + 2), IT = (N + NT - 1) / NT;
-#pragma unroll
-        for (int it = 0; it < IT; ++it) {
-            const int q = threadIdx.x + it * NT;
-            if (q < N) {
-                const int r = 1 + q / W, c = 1 + q % W;
-                const int s = r * RW + c;
-                const double gg = __ldg(gh + off + (long long)r * g.ld + c);
-                double a0[3], a1[3];
-                rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2]);
-                rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2]);
-                const bool inner = r >= H2 && r < H2 + TY && c >= H2 && c < H2 + TX;
-#pragma unroll
-                for (int f = 0; f < 3; ++f) {
-                    const double m0 = a0[f] * dt, m1 = a1[f] * dt;
-                    const double x0 = A[f * RN + s], x1 = B[f * RN + s];
-                    C[f * RN + s] = ((hw.c3[0] * x0 + hw.c3[1] * m0) + hw.c3[2] * x1) + hw.c3[3] * m1;
-                    if (inner)
-                        yh[off + f * g.plane + (long long)r * g.ld + c] =
-                            ((hw.c4[0] * x0 + hw.c4[1] * m0) + hw.c4[2] * x1) + hw.c4[3] * m1;
-                }
-            }
-        }
-    }
-    __syncthreads();
-    // y3 outside the grown tile is never read: stencils of tile cells reach one
-    // cell out.  Cells of C on the outer ring stay unset and unused.
-    {
-        constexpr int N = TX * TY, IT = (N + NT - 1) / NT;
-#pragma unroll
-        for (int it = 0; it < IT; ++it) {
-            const int q = threadIdx.x + it * NT;
-            if (q < N) {
-                const int r = H2 + q / TX, c = H2 + q % TX;
-                const int s = r * RW + c;
-                const double gg = __ldg(gh + off + (long long)r * g.ld + c);
-                double m2[3];
-                rhs_at<RW, RN>(P, C, s, E3 * gg, m2[0], m2[1], m2[2]);
-#pragma unroll
-                for (int f = 0; f < 3; ++f) {
-                    double* p = yh + off + f * g.plane + (long long)r * g.ld + c;
-                    *p = *p + hw.c2 * (m2[f] * dt);
-                }
-            }
-        }
-    }
-}
-
-// Fixed-order block sum (warp shuffles, then warps in order); result valid in
-// thread 0.
-template <int NT>
-__device__ __forceinline__ double block_sum(double v, double* red) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) red[wid] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int w = 0; w < NT / 32; ++w) s += red[w];
-    }
-    return s;
-}
-
-// One backward RK4 step of the reference adjoint (cu-G:1349-1427 in the order
-// of cu-G:1885-1891): stage 1 uses y(t_i) = yb, stages 2-3 the midpoint yh,
-// stage 4 y(t_{i-1}) = ya; z <- z + dz + dt/6 k4.  The tile's share of
-// z_u . gh (NaN terms skipped) goes to partial[tile] (cu-G:1457-1483).
-template <int E, int TX, int TY, int NT, int MODE>
-__device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, double* __restrict__ Zs,
-                                          const double* __restrict__ Z0, double* __restrict__ D,
-                                          const uint8_t* __restrict__ wc, const double* __restrict__ ys,
-                                          long long off, double cZ, double cD, double* __restrict__ out,
-                                          const double* __restrict__ ghs, double& zgh) {
-    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
-    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
-    constexpr int IT = (N + NT - 1) / NT;
-    constexpr int IN = TX * TY;
-    double ku[IT], kv[IT], kw[IT];
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int q = threadIdx.x + it * NT;
-        if (q < N) {
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
+        constexpr int W = TX + 2, N = W * (TY + 2);
+#pragma unroll 1
+        for (int q = threadIdx.x; q < N; q += NT) {
+            const int r = 1 + q / W, c = 1 + q % W;
             const int s = r * RW + c;
             const long long o = off + (long long)r * g.ld + c;
-            const int code = __ldg(wc + o);
-            if (isnan(Zs[s])) {
-                ku[it] = kv[it] = kw[it] = __longlong_as_double(0x7ff8000000000000LL);
-            } else {
-                const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
-                adj_at<RW, RN>(P, Zs, s, code, J, ku[it], kv[it], kw[it]);
+            const double gg = __ldg(gh + o);
+            double a0[3], a1[3];
+            rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2]);
+            rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2]);
+            const bool inner = r >= H2 && r < H2 + TY && c >= H2 && c < H2 + TX;
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                const double m0 = a0[f] * dt, m1 = a1[f] * dt;
+                const double x0 = A[f * RN + s], x1 = B[f * RN + s];
+                C[f * RN + s] = ((hw.c3[0] * x0 + hw.c3[1] * m0) + hw.c3[2] * x1) + hw.c3[3] * m1;
+                if (inner)
+                    yh[o + f * g.plane] = ((hw.c4[0] * x0 + hw.c4[1] * m0) + hw.c4[2] * x1) + hw.c4[3] * m1;
             }
         }
     }
-    if (MODE != 2) __syncthreads();
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int q = threadIdx.x + it * NT;
-        if (q < N) {
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
+    __syncthreads();
+    // C on the outer ring stays unset: stencils of tile cells reach one cell out.
+    {
+        constexpr int N = TX * TY;
+#pragma unroll 1
+        for (int q = threadIdx.x; q < N; q += NT) {
+            const int r = H2 + q / TX, c = H2 + q % TX;
             const int s = r * RW + c;
-            const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
-            const int d = (r - HALO) * TX + (c - HALO);
-            if (MODE == 2) {
-                const long long o = (long long)r * g.ld + c;
-                const double nu = (Z0[s] + D[d]) + cD * ku[it];
-                out[o] = nu;
-                out[g.plane + o] = (Z0[RN + s] + D[IN + d]) + cD * kv[it];
-                out[2 * g.plane + o] = (Z0[2 * RN + s] + D[2 * IN + d]) + cD * kw[it];
-                const double t = nu * __ldg(ghs + o);
-                if (!isnan(t)) zgh += t;
-            } else {
-                Zs[s] = Z0[s] + cZ * ku[it];
-                Zs[RN + s] = Z0[RN + s] + cZ * kv[it];
-                Zs[2 * RN + s] = Z0[2 * RN + s] + cZ * kw[it];
-                if (inner) {
-                    if (MODE == 0) {
-                        D[d] = cD * ku[it];
-                        D[IN + d] = cD * kv[it];
-                        D[2 * IN + d] = cD * kw[it];
-                    } else {
-                        D[d] = D[d] + cD * ku[it];
-                        D[IN + d] = D[IN + d] + cD * kv[it];
-                        D[2 * IN + d] = D[2 * IN + d] + cD * kw[it];
-                    }
+            const long long o = off + (long long)r * g.ld + c;
+            double m2[3];
+            rhs_at<RW, RN>(P, C, s, E3 * __ldg(gh + o), m2[0], m2[1], m2[2]);
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                double* p = yh + o + f * g.plane;
+                *p = *p + hw.c2 * (m2[f] * dt);
+            }
+        }
+    }
+}
+
+// One adjoint stage on the tile grown by E cells: k = L^T src + J_F(y)^T src,
+// then (reference mode)
+//   MODE 0: dst = z0 + cZ*k, D  = cD*k
+//   MODE 1: dst = z0 + cZ*k, D += cD*k
+//   MODE 2: out = (z0 + D) + cD*k; D_u <- out_u * gh (0 where NaN), the cell's
+//           term of z.gh, which subblock_sums reduces afterwards
+// (cu-G:1349-1427 in the order of cu-G:1885-1891).
+template <int E, int TX, int TY, int NT, int MODE>
+__device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, const double* __restrict__ src,
+                                          double* __restrict__ dst, double* __restrict__ D,
+                                          const double* __restrict__ z0g, const uint8_t* __restrict__ wc,
+                                          const double* __restrict__ ys, long long off, double cZ, double cD,
+                                          double* __restrict__ out, const double* __restrict__ gh) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
+    constexpr int IN = TX * TY;
+#pragma unroll 1
+    for (int q = threadIdx.x; q < N; q += NT) {
+        const int r = HALO - E + q / W, c = HALO - E + q % W;
+        const int s = r * RW + c;
+        const long long o = off + (long long)r * g.ld + c;
+        double ku, kv, kw;
+        if (isnan(src[s])) {
+            ku = kv = kw = kNaN;
+        } else {
+            const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+            adj_at<RW, RN>(P, src, s, __ldg(wc + o), J, ku, kv, kw);
+        }
+        const double a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
+        const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+        const int d = (r - HALO) * TX + (c - HALO);
+        if (MODE == 2) {
+            const double nu = (a + D[d]) + cD * ku;
+            out[o] = nu;
+            out[g.plane + o] = (b + D[IN + d]) + cD * kv;
+            out[2 * g.plane + o] = (e + D[2 * IN + d]) + cD * kw;
+            const double t = nu * __ldg(gh + o);
+            D[d] = isnan(t) ? 0.0 : t;
+        } else {
+            dst[s] = a + cZ * ku;
+            dst[RN + s] = b + cZ * kv;
+            dst[2 * RN + s] = e + cZ * kw;
+            if (inner) {
+                if (MODE == 0) {
+                    D[d] = cD * ku;
+                    D[IN + d] = cD * kv;
+                    D[2 * IN + d] = cD * kw;
+                } else {
+                    D[d] = D[d] + cD * ku;
+                    D[IN + d] = D[IN + d] + cD * kv;
+                    D[2 * IN + d] = D[2 * IN + d] + cD * kw;
                 }
             }
         }
@@ -307,35 +313,32 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, d
     if (MODE != 2) __syncthreads();
 }
 
+// One backward RK4 step of the reference adjoint: stage 1 uses y(t_i) = yb,
+// stages 2-3 the midpoint yh, stage 4 y(t_{i-1}) = ya; the tile's 16x16
+// sub-block sums of z_u . gh (NaN terms skipped, cu-G:1457-1483) go to `row`.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z,
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z,
                                                  double* __restrict__ zout, const double* __restrict__ yb,
                                                  const double* __restrict__ yh, const double* __restrict__ ya,
                                                  const uint8_t* __restrict__ wc, const double* __restrict__ gh,
-                                                 double* __restrict__ partial) {
+                                                 double* __restrict__ row, int nsbx) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
-    constexpr int IN = TX * TY;
     extern __shared__ double4 smem_raw[];
-    double* Zs = reinterpret_cast<double*>(smem_raw);
-    double* Z0 = Zs + 3 * RN;
-    double* D = Z0 + 3 * RN;
-    double* red = D + 3 * IN;
+    double* A = reinterpret_cast<double*>(smem_raw);
+    double* B = A + 3 * RN;
+    double* D = B + 3 * RN;
     const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(Zs, z + off, g.ld, g.plane, vec_ok);
-    __syncthreads();
-    for (int q = threadIdx.x; q < 3 * RN; q += NT) Z0[q] = Zs[q];
+    load_region<RH, RW, NT>(A, z + off, g.ld, g.plane, vec_ok);
     __syncthreads();
     const double dt = P.dt;
-    double zgh = 0.0;
-    const uint8_t* wco = wc;  // byte codes, same padded layout (plane-less)
-    adj_stage<3, TX, TY, NT, 0>(P, g, Zs, Z0, D, wco, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, nullptr, zgh);
-    adj_stage<2, TX, TY, NT, 1>(P, g, Zs, Z0, D, wco, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, nullptr, zgh);
-    adj_stage<1, TX, TY, NT, 1>(P, g, Zs, Z0, D, wco, yh, off, dt, 2.0 / 6.0 * dt, nullptr, nullptr, zgh);
-    adj_stage<0, TX, TY, NT, 2>(P, g, Zs, Z0, D, wco, ya, off, 0.0, 1.0 / 6.0 * dt, zout + off, gh + off, zgh);
-    const double s = block_sum<NT>(zgh, red);
-    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+    adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh);
+    adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh);
+    adj_stage<1, TX, TY, NT, 1>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh);
+    adj_stage<0, TX, TY, NT, 2>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh);
+    __syncthreads();
+    subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
 }
 
 // ------------------------------------------------------ exact-mode adjoint
@@ -351,63 +354,49 @@ __global__ void __launch_bounds__(NT) k_adj_step(DevModel P, DevGrid g, const do
 // b.a4 (sample s+1), b = gh on u.  Same temporal blocking as the reference
 // mode: a_s lives in shared memory on the tile grown by (4 - s) cells.
 template <int E, int TX, int TY, int NT, int MODE>
-__device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g, double* __restrict__ A,
-                                            const double* __restrict__ L0, double* __restrict__ D,
-                                            const uint8_t* __restrict__ wc, const double* __restrict__ ys,
-                                            long long off, double cL, double cM, double* __restrict__ out,
-                                            const double* __restrict__ ghs, double& acc) {
+__device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g, const double* __restrict__ src,
+                                            double* __restrict__ dst, double* __restrict__ D,
+                                            const double* __restrict__ lamg, const uint8_t* __restrict__ wc,
+                                            const double* __restrict__ ys, long long off, double cL, double cM,
+                                            double* __restrict__ out, double* __restrict__ keep_u) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
-    constexpr int IT = (N + NT - 1) / NT;
     constexpr int IN = TX * TY;
-    double ku[IT], kv[IT], kw[IT];
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int q = threadIdx.x + it * NT;
-        if (q < N) {
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
-            const int s = r * RW + c;
-            const long long o = off + (long long)r * g.ld + c;
-            if (isnan(A[s])) {
-                ku[it] = kv[it] = kw[it] = A[s];
-            } else {
-                const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
-                adj_at<RW, RN>(P, A, s, __ldg(wc + o), J, ku[it], kv[it], kw[it]);
-            }
+#pragma unroll 1
+    for (int q = threadIdx.x; q < N; q += NT) {
+        const int r = HALO - E + q / W, c = HALO - E + q % W;
+        const int s = r * RW + c;
+        const long long o = off + (long long)r * g.ld + c;
+        double ku, kv, kw;
+        if (isnan(src[s])) {
+            ku = kv = kw = kNaN;
+        } else {
+            const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+            adj_at<RW, RN>(P, src, s, __ldg(wc + o), J, ku, kv, kw);
         }
-    }
-    if (MODE != 2) __syncthreads();
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int q = threadIdx.x + it * NT;
-        if (q < N) {
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
-            const int s = r * RW + c;
-            const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
-            const int d = (r - HALO) * TX + (c - HALO);
-            if (MODE == 2) {
-                const long long o = (long long)r * g.ld + c;
-                out[o] = L0[s] + (D[d] + ku[it]);
-                out[g.plane + o] = L0[RN + s] + (D[IN + d] + kv[it]);
-                out[2 * g.plane + o] = L0[2 * RN + s] + (D[2 * IN + d] + kw[it]);
-            } else {
-                const double au = cL * L0[s] + cM * ku[it];
-                A[s] = au;
-                A[RN + s] = cL * L0[RN + s] + cM * kv[it];
-                A[2 * RN + s] = cL * L0[2 * RN + s] + cM * kw[it];
-                if (inner) {
-                    if (MODE == 0) {
-                        D[d] = ku[it];
-                        D[IN + d] = kv[it];
-                        D[2 * IN + d] = kw[it];
-                    } else {
-                        D[d] = D[d] + ku[it];
-                        D[IN + d] = D[IN + d] + kv[it];
-                        D[2 * IN + d] = D[2 * IN + d] + kw[it];
-                    }
-                    const double t = au * __ldg(ghs + (long long)r * g.ld + c);
-                    if (!isnan(t)) acc += t;
+        const double la = __ldg(lamg + o), lb = __ldg(lamg + g.plane + o), lc = __ldg(lamg + 2 * g.plane + o);
+        const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+        const int d = (r - HALO) * TX + (c - HALO);
+        if (MODE == 2) {
+            out[o] = la + (D[d] + ku);
+            out[g.plane + o] = lb + (D[IN + d] + kv);
+            out[2 * g.plane + o] = lc + (D[2 * IN + d] + kw);
+        } else {
+            const double au = cL * la + cM * ku;
+            dst[s] = au;
+            dst[RN + s] = cL * lb + cM * kv;
+            dst[2 * RN + s] = cL * lc + cM * kw;
+            if (inner) {
+                if (MODE == 0) {
+                    D[d] = ku;
+                    D[IN + d] = kv;
+                    D[2 * IN + d] = kw;
+                } else {
+                    D[d] = D[d] + ku;
+                    D[IN + d] = D[IN + d] + kv;
+                    D[2 * IN + d] = D[2 * IN + d] + kw;
                 }
+                if (keep_u) keep_u[d] = au;
             }
         }
     }
@@ -416,67 +405,65 @@ __device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g,
 
 // lam (state of lambda_{s+1}) -> lamout (lambda_s); y = y_s; stages = Y2, Y3,
 // Y4 of step s (three consecutive states, written by k_fwd_step).
-// Per tile: p1 <- b.a1, p23 <- b.(a2 + a3), p4 <- b.a4.
+// 16x16 sub-block sums: r1 <- b.a1, r23 <- b.(a2 + a3), r4 <- b.a4.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) k_adj_exact(DevModel P, DevGrid g, const double* __restrict__ lam,
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_exact(DevModel P, DevGrid g, const double* __restrict__ lam,
                                                   double* __restrict__ lamout, const double* __restrict__ y,
                                                   const double* __restrict__ stages,
                                                   const uint8_t* __restrict__ wc, const double* __restrict__ gh,
-                                                  double* __restrict__ p1, double* __restrict__ p23,
-                                                  double* __restrict__ p4) {
+                                                  double* __restrict__ r1, double* __restrict__ r23,
+                                                  double* __restrict__ r4, int nsbx) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int IN = TX * TY;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
-    double* L0 = A + 3 * RN;
-    double* D = L0 + 3 * RN;
-    double* red = D + 3 * IN;
+    double* B = A + 3 * RN;
+    double* D = B + 3 * RN;
+    double* T3 = D + 3 * IN;  // a3_u on the tile
     const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(L0, lam + off, g.ld, g.plane, vec_ok);
+    load_region<RH, RW, NT>(A, lam + off, g.ld, g.plane, vec_ok);
     __syncthreads();
     const double dt = P.dt;
     const double c6 = dt / 6.0, c3 = dt / 3.0, c2 = dt * 0.5;
-    for (int q = threadIdx.x; q < 3 * RN; q += NT) A[q] = c6 * L0[q];
-    // b.a4 over the tile
-    const double* ghs = gh + off;
-    double acc4 = 0.0, acc23 = 0.0, acc1 = 0.0;
-    for (int q = threadIdx.x; q < IN; q += NT) {
-        const int r = HALO + q / TX, c = HALO + q % TX;
-        const double t = c6 * L0[r * RW + c] * __ldg(ghs + (long long)r * g.ld + c);
-        if (!isnan(t)) acc4 += t;
-    }
+#pragma unroll 2
+    for (int q = threadIdx.x; q < 3 * RN; q += NT) A[q] = c6 * A[q];  // a4
     __syncthreads();
     const long long sst = 3 * g.plane;
-    exact_stage<3, TX, TY, NT, 0>(P, g, A, L0, D, wc, stages + 2 * sst, off, c3, dt, nullptr, ghs, acc23);
-    exact_stage<2, TX, TY, NT, 1>(P, g, A, L0, D, wc, stages + sst, off, c3, c2, nullptr, ghs, acc23);
-    exact_stage<1, TX, TY, NT, 1>(P, g, A, L0, D, wc, stages, off, c6, c2, nullptr, ghs, acc1);
-    exact_stage<0, TX, TY, NT, 2>(P, g, A, L0, D, wc, y, off, 0.0, 0.0, lamout + off, ghs, acc1);
-    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
-    double s = block_sum<NT>(acc1, red);
-    if (threadIdx.x == 0) p1[tile] = s;
-    s = block_sum<NT>(acc23, red);
-    if (threadIdx.x == 0) p23[tile] = s;
-    s = block_sum<NT>(acc4, red);
-    if (threadIdx.x == 0) p4[tile] = s;
+    exact_stage<3, TX, TY, NT, 0>(P, g, A, B, D, lam, wc, stages + 2 * sst, off, c3, dt, nullptr, T3);
+    exact_stage<2, TX, TY, NT, 1>(P, g, B, A, D, lam, wc, stages + sst, off, c3, c2, nullptr, nullptr);
+    exact_stage<1, TX, TY, NT, 1>(P, g, A, B, D, lam, wc, stages, off, c6, c2, nullptr, nullptr);
+    exact_stage<0, TX, TY, NT, 2>(P, g, B, A, D, lam, wc, y, off, 0.0, 0.0, lamout, nullptr);
+    __syncthreads();
+    // now A holds a2 and B holds a1 on the tile
+    auto ghv = [&](int r, int c) { return __ldg(gh + off + (long long)(r + HALO) * g.ld + (c + HALO)); };
+    auto z0 = [](double t) { return isnan(t) ? 0.0 : t; };
+    subblock_sums<TX, TY, NT>([&](int r, int c) { return z0(B[(r + HALO) * RW + c + HALO] * ghv(r, c)); },
+                              r1, i0, j0, nsbx);
+    subblock_sums<TX, TY, NT>(
+        [&](int r, int c) { return z0((A[(r + HALO) * RW + c + HALO] + T3[r * TX + c]) * ghv(r, c)); }, r23, i0,
+        j0, nsbx);
+    subblock_sums<TX, TY, NT>(
+        [&](int r, int c) {
+            return z0(c6 * __ldg(lam + off + (long long)(r + HALO) * g.ld + (c + HALO)) * ghv(r, c));
+        },
+        r4, i0, j0, nsbx);
 }
 
-// z_u . gh over one tile (NaN terms skipped) -> partial[tile].
-template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) k_dot_gh(DevGrid g, const double* __restrict__ z,
-                                               const double* __restrict__ gh, double* __restrict__ partial) {
-    __shared__ double red[NT / 32];
-    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
-    double acc = 0.0;
-    for (int q = threadIdx.x; q < TX * TY; q += NT) {
-        const int r = q / TX, c = q % TX;
-        const long long o = (long long)(i0 + HALO + r) * g.ld + (j0 + HALO + c);
-        const double t = z[o] * gh[o];
-        if (!isnan(t)) acc += t;
-    }
-    const double s = block_sum<NT>(acc, red);
-    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+// z_u . gh per 16x16 sub-block (NaN terms skipped), one warp per sub-block,
+// in the order of subblock_sums -> row[sub-block].
+__global__ void __launch_bounds__(32) k_dot_gh(DevGrid g, const double* __restrict__ z,
+                                               const double* __restrict__ gh, double* __restrict__ row,
+                                               int nsbx) {
+    const int b = blockIdx.x, by = b / nsbx, bx = b - by * nsbx;
+    subblock_sums<16, 16, 32>(
+        [&](int r, int c) {
+            const long long o = (long long)(by * 16 + r + HALO) * g.ld + (bx * 16 + c + HALO);
+            const double t = z[o] * gh[o];
+            return isnan(t) ? 0.0 : t;
+        },
+        row, by * 16, bx * 16, nsbx);
 }
 
 // out[row] = sum_k partial[row*ntiles + k], fixed order (one block per row).
@@ -545,60 +532,75 @@ __global__ void k_objective(const double* __restrict__ yc, int n_num, const long
 
 // --------------------------------------------------------------- launchers
 
-template <int TX, int TY, int NT>
-static size_t fwd_smem() {
+// two 3-field region buffers + the 3-field interior accumulator; the exact
+// adjoint keeps one more interior plane (a3_u)
+template <int TX, int TY>
+static size_t stencil_smem(int /*nt*/) {
     constexpr int RN = (TX + 2 * HALO) * (TY + 2 * HALO);
     return sizeof(double) * (6 * RN + 3 * TX * TY);
 }
-template <int TX, int TY, int NT>
+template <int TX, int TY>
+static size_t exact_smem() {
+    constexpr int RN = (TX + 2 * HALO) * (TY + 2 * HALO);
+    return sizeof(double) * (6 * RN + 4 * TX * TY);
+}
+template <int TX, int TY>
 static size_t mid_smem() {
     constexpr int RN = (TX + 4) * (TY + 4);
     return sizeof(double) * (9 * RN);
-}
-template <int TX, int TY, int NT>
-static size_t adj_smem() {
-    constexpr int RN = (TX + 2 * HALO) * (TY + 2 * HALO);
-    return sizeof(double) * (6 * RN + 3 * TX * TY + NT / 32);
 }
 
 template <int TX, int TY, int NT>
 static cudaError_t setup_tile() {
     cudaError_t e;
-    e = cudaFuncSetAttribute(k_fwd_step<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem<TX, TY, NT>());
-    if (e) return e;
-    e = cudaFuncSetAttribute(k_adj_mid<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid_smem<TX, TY, NT>());
-    if (e) return e;
-    e = cudaFuncSetAttribute(k_adj_exact<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem<TX, TY, NT>());
-    if (e) return e;
-    return cudaFuncSetAttribute(k_adj_step<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem<TX, TY, NT>());
+    const int s = (int)stencil_smem<TX, TY>(NT);
+    if ((e = cudaFuncSetAttribute(k_fwd_step<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s))) return e;
+    if ((e = cudaFuncSetAttribute(k_adj_step<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s))) return e;
+    if ((e = cudaFuncSetAttribute(k_adj_exact<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)exact_smem<TX, TY>())))
+        return e;
+    return cudaFuncSetAttribute(k_adj_mid<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)mid_smem<TX, TY>());
 }
 
-#define FKADJ_TILES(X) X(32, 32, 256) X(32, 16, 256) X(64, 32, 512) X(16, 16, 256)
+// Tile presets (TX, TY, threads).  All TY divide 64 (the row padding of the
+// state planes) and all TX are multiples of 16.
+#define FKADJ_TILE_LIST(X) \
+    X(0, 32, 32, 256)      \
+    X(1, 32, 32, 512)      \
+    X(2, 64, 32, 512)      \
+    X(3, 32, 16, 256)      \
+    X(4, 16, 16, 256)      \
+    X(5, 64, 16, 512)
 
-int tile_count() { return 4; }
+int tile_count() { return 6; }
 
 TileShape tile_shape(int t) {
     switch (t) {
-        case 1: return {32, 16, 256};
-        case 2: return {64, 32, 512};
-        case 3: return {16, 16, 256};
+#define X(id, a, b, c) \
+    case id: return {a, b, c};
+        FKADJ_TILE_LIST(X)
+#undef X
         default: return {32, 32, 256};
     }
 }
 
 cudaError_t kernels_init() {
     cudaError_t e;
-#define X(a, b, c) if ((e = setup_tile<a, b, c>()) != cudaSuccess) return e;
-    FKADJ_TILES(X)
+#define X(id, a, b, c) \
+    if ((e = setup_tile<a, b, c>()) != cudaSuccess) return e;
+    FKADJ_TILE_LIST(X)
 #undef X
     return cudaSuccess;
 }
 
-#define DISPATCH(tile, CALL)                                           \
-    switch (tile) {                                                    \
-        case 1: { constexpr int TX = 32, TY = 16, NT = 256; CALL; } break; \
+#define DISPATCH(tile, CALL)                              \
+    switch (tile) {                                       \
+        case 1: { constexpr int TX = 32, TY = 32, NT = 512; CALL; } break; \
         case 2: { constexpr int TX = 64, TY = 32, NT = 512; CALL; } break; \
-        case 3: { constexpr int TX = 16, TY = 16, NT = 256; CALL; } break; \
+        case 3: { constexpr int TX = 32, TY = 16, NT = 256; CALL; } break; \
+        case 4: { constexpr int TX = 16, TY = 16, NT = 256; CALL; } break; \
+        case 5: { constexpr int TX = 64, TY = 16, NT = 512; CALL; } break; \
         default: { constexpr int TX = 32, TY = 32, NT = 256; CALL; } break; \
     }
 
@@ -609,39 +611,44 @@ static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, double E0, double Eh, double E1, cudaStream_t st,
                             double* stages) {
-    DISPATCH(tile, (k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, fwd_smem<TX, TY, NT>(), st>>>(
+    DISPATCH(tile, (k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT), st>>>(
                         P, g, yin, yout, gh, E0, Eh, E1, stages)));
     return cudaGetLastError();
 }
 
 cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, const double* lam, double* lamout,
                              const double* y, const double* stages, const uint8_t* wc, const double* gh,
-                             double* p1, double* p23, double* p4, cudaStream_t st) {
-    DISPATCH(tile, (k_adj_exact<TX, TY, NT><<<tile_grid(g, TX, TY), NT, adj_smem<TX, TY, NT>(), st>>>(
-                        P, g, lam, lamout, y, stages, wc, gh, p1, p23, p4)));
+                             double* r1, double* r23, double* r4, int nsbx, cudaStream_t st) {
+    DISPATCH(tile, (k_adj_exact<TX, TY, NT><<<tile_grid(g, TX, TY), NT, exact_smem<TX, TY>(), st>>>(
+                        P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx)));
     return cudaGetLastError();
 }
 
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
                            cudaStream_t st) {
-    DISPATCH(tile, (k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, TY), NT, mid_smem<TX, TY, NT>(), st>>>(
+    DISPATCH(tile, (k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, TY), NT, mid_smem<TX, TY>(), st>>>(
                         P, g, ya, yb, gh, yh, Ea, Eb, E3, hw)));
     return cudaGetLastError();
 }
 
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
-                            const double* gh, double* partial, cudaStream_t st) {
-    DISPATCH(tile, (k_adj_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, adj_smem<TX, TY, NT>(), st>>>(
-                        P, g, z, zout, yb, yh, ya, wc, gh, partial)));
+                            const double* gh, double* row, int nsbx, cudaStream_t st) {
+    DISPATCH(tile, (k_adj_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT), st>>>(
+                        P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_dot_gh(int tile, const DevGrid& g, const double* z, const double* gh, double* partial,
+cudaError_t launch_dot_gh(const DevGrid& g, const double* z, const double* gh, double* row, int nsbx, int nsby,
                           cudaStream_t st) {
-    DISPATCH(tile, (k_dot_gh<TX, TY, NT><<<tile_grid(g, TX, TY), NT, 0, st>>>(g, z, gh, partial)));
+    k_dot_gh<<<nsbx * nsby, 32, 0, st>>>(g, z, gh, row, nsbx);
     return cudaGetLastError();
+}
+
+void subblock_lattice(const DevGrid& g, int* nsbx, int* nsby) {
+    *nsbx = ((g.ncols + 63) / 64) * 4;
+    *nsby = ((g.nrows + 63) / 64) * 4;
 }
 
 int tiles_of(int tile, const DevGrid& g) {

@@ -27,16 +27,20 @@ cudaError_t kernels_init();
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, double E0, double Eh, double E1, cudaStream_t st,
                             double* stages = nullptr);
+// The z.gh style reductions write one partial per 16x16 sub-block of the
+// grid's lattice (nsbx x nsby, covering the 64-padded grid); sub-blocks no
+// tile covers are never written and must be zero.
+void subblock_lattice(const DevGrid& g, int* nsbx, int* nsby);
 cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, const double* lam, double* lamout,
                              const double* y, const double* stages, const uint8_t* wc, const double* gh,
-                             double* p1, double* p23, double* p4, cudaStream_t st);
+                             double* r1, double* r23, double* r4, int nsbx, cudaStream_t st);
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
                            cudaStream_t st);
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
-                            const double* gh, double* partial, cudaStream_t st);
-cudaError_t launch_dot_gh(int tile, const DevGrid& g, const double* z, const double* gh, double* partial,
+                            const double* gh, double* row, int nsbx, cudaStream_t st);
+cudaError_t launch_dot_gh(const DevGrid& g, const double* z, const double* gh, double* row, int nsbx, int nsby,
                           cudaStream_t st);
 cudaError_t launch_sum_rows(const double* partial, int rows, int ntiles, double* out, cudaStream_t st);
 cudaError_t launch_scatter(const DevGrid& g, const double* yc, int n_num, const long long* pos, double scale,

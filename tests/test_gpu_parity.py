@@ -40,15 +40,31 @@ def test_forward_matches_oracle(shape):
     assert "h = 0.025" in pstr
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3])
+@pytest.mark.parametrize("tile", [1, 2, 3, 4, 5, 6])
 def test_forward_state_is_independent_of_tile_shape(tile):
+    """options.tile k >= 1 fixes preset k-1 for every kernel; 0 autotunes."""
     inst = _inst(96, 40, seed=3, ncols=72)
     ref = api.fk_forward_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
-                            inst.ghost, 40, params=inst.params, opts=api.options(tile=0))[1]
+                            inst.ghost, 40, params=inst.params, opts=api.options(tile=1))[1]
     yf = api.fk_forward_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
                            inst.ghost, 40, params=inst.params, opts=api.options(tile=tile))[1]
     assert np.array_equal(np.isnan(ref), np.isnan(yf))
     assert np.array_equal(ref[~np.isnan(ref)], yf[~np.isnan(yf)])
+
+
+@pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
+def test_gradient_bits_are_independent_of_tile_and_autotune(mode):
+    """Fixed-order 16x16 sub-block reductions: every tile preset and the
+    autotuned choice give bit-identical gradients."""
+    inst = _inst(80, 60, seed=13, ncols=112, objective="gradient")
+    outs = []
+    for tile in (0, 1, 2, 3, 4, 5, 6):
+        outs.append(api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols,
+                                   inst.nrows, inst.ghost, inst.gamma, inst.S, 0.1, params=inst.params,
+                                   opts=api.options(tile=tile, grad_mode=mode)))
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0])
+        assert o[1] == outs[0][1]
 
 
 @pytest.mark.parametrize("objective", ["mean_u2", "gradient"])
