@@ -157,6 +157,25 @@ int64_t fkadj_problem_last_launches(const fkadj_problem *pb);
 void fkadj_problem_set_profiling(fkadj_problem *pb, int enable);
 void fkadj_problem_kernel_time(const fkadj_problem *pb, int kernel, double *avg_ms, int64_t *samples);
 
+/* ------------------------------------------------------------------------
+ * z.gh without allocating.  No counterpart in the reference: it is the
+ * reduction the reference takes once per backward step (sum of z_u * gh over
+ * the grid, NaN terms skipped), offered to callers that cannot call
+ * cudaMalloc -- their device memory belongs to another allocator or pool, or
+ * they must not pay cudaMalloc/cudaFree inside a timed loop.
+ *   d_zu, d_gh  device arrays, dense row-major nrows x ncols (NaN at holes)
+ *   d_out       device double that receives the sum (written on `stream`)
+ * The partial sums use a fixed device array of FKADJ_NOALLOC_MAX_SUBBLOCKS
+ * 16x16 sub-blocks (512 KiB, held by every GPU that loads the library until
+ * exit); larger grids are rejected with FKADJ_ERR_ARG.  The first call on a
+ * device resolves that array's address (make it before any stream capture).
+ * All calls on a device share the array: calls that overlap on the GPU race,
+ * so the caller serialises them.  Nothing is allocated.
+ * --------------------------------------------------------------------- */
+#define FKADJ_NOALLOC_MAX_SUBBLOCKS 65536
+fkadj_status fkadj_zgh_dot_noalloc(const double *d_zu, const double *d_gh, int nrows, int ncols, double *d_out,
+                                   void *stream);
+
 #ifdef __cplusplus
 }
 #endif
