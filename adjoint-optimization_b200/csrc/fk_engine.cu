@@ -242,7 +242,7 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
 
 int64_t Problem::device_bytes() const {
     const DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_,
-                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &y0res_, &stg_};
+                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &y0res_, &stg_, &jcache_, &fcache_};
     int64_t s = 0;
     for (auto* b : all) s += (int64_t)b->bytes;
     return s;
@@ -500,6 +500,11 @@ fkadj_status Problem::ensure_adjoint_work() {
     if (grad_mode_ == FKADJ_GRAD_REF && !yh_.p) {
         CK(yh_.alloc(state_bytes()), "alloc midpoint state");
         CK(cudaMemsetAsync(yh_.p, 0xff, yh_.bytes, st_), "init midpoint state");
+        // Jacobian caches J(y) x2 and J(yh) (7 planes each), f(y) carry x2 (3 planes each)
+        CK(jcache_.alloc(21 * (size_t)g_.plane * sizeof(double)), "alloc Jacobian cache");
+        CK(cudaMemsetAsync(jcache_.p, 0xff, jcache_.bytes, st_), "init Jacobian cache");
+        CK(fcache_.alloc(6 * (size_t)g_.plane * sizeof(double)), "alloc f cache");
+        CK(cudaMemsetAsync(fcache_.p, 0xff, fcache_.bytes, st_), "init f cache");
     }
     if (grad_mode_ == FKADJ_GRAD_EXACT && !stg_.p) {
         CK(stg_.alloc(3 * state_bytes()), "alloc stage states");
@@ -548,13 +553,18 @@ fkadj_status Problem::autotune() {
     });
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_REF) {
         double* z2 = zbuf_.as<double>() + state_elems();
+        const size_t pl = (size_t)g_.plane;
+        double* jc = jcache_.as<double>();
+        double* fc = fcache_.as<double>();
+        // trial launches with the caches in use, as in the backward sweep
         e = pick(T_MID, [&](int t) {
-            return launch_adj_mid(t, P_, g_, y, y, gh_.as<double>(), yh_.as<double>(), E, E, E, hw_, st_);
+            return launch_adj_mid(t, P_, g_, y, y, gh_.as<double>(), yh_.as<double>(), E, E, E, hw_, st_, fc,
+                                  fc + 3 * pl, jc + 14 * pl);
         });
         if (!e)
             e = pick(T_ADJ, [&](int t) {
                 return launch_adj_step(t, P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
-                                       partial_.as<double>(), nsbx_, st_);
+                                       partial_.as<double>(), nsbx_, st_, jc, jc + 14 * pl, jc + 7 * pl);
             });
     }
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_EXACT) {
@@ -678,19 +688,32 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         launches_ += 2;
     }
     // ---- backward sweep (cu-G:1866-1908)
+    // Work carried from backward step i to step i-1 (computed once, same
+    // values): f(y_{i-1}, Et[i-1]) from the midpoint kernel and J(y_{i-1})^T
+    // from the adjoint step's last stage; both ping-pong between two buffers.
+    const size_t pl = (size_t)g_.plane;
+    double* jy[2] = {jcache_.as<double>(), jcache_.as<double>() + 7 * pl};
+    double* jh = jcache_.as<double>() + 14 * pl;
+    double* fc[2] = {fcache_.as<double>(), fcache_.as<double>() + 3 * pl};
+    bool have_carry = false;
+    int cur_c = 0;
     auto back_step = [&](int i, const double* ya, const double* yb) -> fkadj_status {
+        const int nxt = 1 - cur_c;
         CK(prof_begin(K_MID), "profiling event");
         CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), Et_[i - 1], Et_[i],
-                          E3_[i - 1], hw_, st_),
+                          E3_[i - 1], hw_, st_, have_carry ? fc[cur_c] : nullptr, fc[nxt], jh),
            "adjoint midpoint");
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
-                           gh_.as<double>(), part + (size_t)(i - 1) * nsb, nsbx_, st_),
+                           gh_.as<double>(), part + (size_t)(i - 1) * nsb, nsbx_, st_,
+                           have_carry ? jy[cur_c] : nullptr, jh, jy[nxt]),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
         std::swap(z, z2);
+        cur_c = nxt;
+        have_carry = true;
         return FKADJ_OK;
     };
     if (exact) {

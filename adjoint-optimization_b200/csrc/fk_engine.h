@@ -139,6 +139,8 @@ private:
     DevBuf traj_, seg_;
     DevBuf y0res_;     // resident initial state
     DevBuf stg_;       // stage states Y2, Y3, Y4 of one step (exact mode)
+    DevBuf jcache_;    // cached Jacobians (reference mode): J(y) ping-pong + J(yh)
+    DevBuf fcache_;    // f(y) carried between backward steps (reference mode)
     bool have_y0_ = false;
     TrajPlan traj_plan_{};
 

@@ -26,6 +26,13 @@ namespace {
 
 constexpr double kNaN = __builtin_nan("");
 
+// Cells a thread keeps in flight per stage loop iteration (independent FP64
+// chains the scheduler can interleave).
+#ifndef FKADJ_STAGE_UNROLL
+#define FKADJ_STAGE_UNROLL 1
+#endif
+constexpr int kStageUnroll = FKADJ_STAGE_UNROLL;
+
 // Resident CTAs per SM the register allocation targets: what shared memory
 // allows for the tile (101 KB at 32x32, 58 KB at 32x16 and below, one
 // 512-thread CTA).
@@ -117,14 +124,16 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
     constexpr int IN = TX * TY;
-#pragma unroll 1
+#pragma unroll kStageUnroll
     for (int q = threadIdx.x; q < N; q += NT) {
         const int r = HALO - E + q / W, c = HALO - E + q % W;
         const int s = r * RW + c;
         const long long o = (long long)r * ld + c;
-        double ku, kv, kw;
-        rhs_at<RW, RN>(P, src, s, Ev * __ldg(ghs + o), ku, kv, kw);
+        // global operands first: their latency overlaps the stencil arithmetic
+        const double gv = __ldg(ghs + o);
         const double a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
+        double ku, kv, kw;
+        rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw);
         const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
@@ -190,15 +199,43 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_fwd_step(DevMode
 
 // ------------------------------------------------- reference-mode adjoint
 
+// Cached Jacobians: the seven entries of J_F(y)^T of every cell, seven planes.
+__device__ __forceinline__ JacT load_jac(const double* __restrict__ Jb, long long plane, long long o) {
+    JacT J;
+    J.a0 = __ldg(Jb + o);
+    J.a1 = __ldg(Jb + plane + o);
+    J.a2 = __ldg(Jb + 2 * plane + o);
+    J.a3 = __ldg(Jb + 3 * plane + o);
+    J.a4 = __ldg(Jb + 4 * plane + o);
+    J.a5 = __ldg(Jb + 5 * plane + o);
+    J.a6 = __ldg(Jb + 6 * plane + o);
+    return J;
+}
+__device__ __forceinline__ void store_jac(double* __restrict__ Jb, long long plane, long long o, const JacT& J) {
+    Jb[o] = J.a0;
+    Jb[plane + o] = J.a1;
+    Jb[2 * plane + o] = J.a2;
+    Jb[3 * plane + o] = J.a3;
+    Jb[4 * plane + o] = J.a4;
+    Jb[5 * plane + o] = J.a5;
+    Jb[6 * plane + o] = J.a6;
+}
+
 // Midpoint state of step [t_{i-1}, t_i] (cu-G:1244-1301): y3 = cubic Hermite
 // at 1/3 from (ya, yb, dt*f(ya), dt*f(yb)); yh = partial quartic at 1/2 plus
 // (27/64) dt f(y3, E(t_{i-1}+dt/3)).  Halo 2: f(ya), f(yb) on the tile grown by
 // one cell, f(y3) on the tile.
+// Work shared between consecutive backward steps (same values, computed once):
+//   f(yb, Eb) of step i is f(ya, Ea) of step i+1: when fin is non-null it is
+//   read from there instead of evaluated, and f(ya, Ea) goes to fout;
+//   J_F(yh)^T, used by stages 2 and 3 of the adjoint step, goes to jh.
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya,
                                                 const double* __restrict__ yb,
                                                 const double* __restrict__ gh, double* __restrict__ yh,
-                                                double Ea, double Eb, double E3, HermiteW hw) {
+                                                double Ea, double Eb, double E3, HermiteW hw,
+                                                const double* __restrict__ fin, double* __restrict__ fout,
+                                                double* __restrict__ jh) {
     constexpr int H2 = 2;
     constexpr int RW = TX + 2 * H2, RH = TY + 2 * H2, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
@@ -215,7 +252,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel
     const double dt = P.dt;
     {
         constexpr int W = TX + 2, N = W * (TY + 2);
-#pragma unroll 1
+#pragma unroll kStageUnroll
         for (int q = threadIdx.x; q < N; q += NT) {
             const int r = 1 + q / W, c = 1 + q % W;
             const int s = r * RW + c;
@@ -223,8 +260,19 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel
             const double gg = __ldg(gh + o);
             double a0[3], a1[3];
             rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2]);
-            rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2]);
+            if (fin) {
+                a1[0] = __ldg(fin + o);
+                a1[1] = __ldg(fin + g.plane + o);
+                a1[2] = __ldg(fin + 2 * g.plane + o);
+            } else {
+                rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2]);
+            }
             const bool inner = r >= H2 && r < H2 + TY && c >= H2 && c < H2 + TX;
+            if (inner && fout) {
+                fout[o] = a0[0];
+                fout[g.plane + o] = a0[1];
+                fout[2 * g.plane + o] = a0[2];
+            }
 #pragma unroll
             for (int f = 0; f < 3; ++f) {
                 const double m0 = a0[f] * dt, m1 = a1[f] * dt;
@@ -239,18 +287,20 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel
     // C on the outer ring stays unset: stencils of tile cells reach one cell out.
     {
         constexpr int N = TX * TY;
-#pragma unroll 1
+#pragma unroll kStageUnroll
         for (int q = threadIdx.x; q < N; q += NT) {
             const int r = H2 + q / TX, c = H2 + q % TX;
             const int s = r * RW + c;
             const long long o = off + (long long)r * g.ld + c;
-            double m2[3];
+            double m2[3], yv[3];
             rhs_at<RW, RN>(P, C, s, E3 * __ldg(gh + o), m2[0], m2[1], m2[2]);
 #pragma unroll
             for (int f = 0; f < 3; ++f) {
                 double* p = yh + o + f * g.plane;
-                *p = *p + hw.c2 * (m2[f] * dt);
+                yv[f] = *p + hw.c2 * (m2[f] * dt);
+                *p = yv[f];
             }
+            if (jh && !isnan(yv[0])) store_jac(jh, g.plane, o, fk_jacT(P, yv[0], yv[1], yv[2]));
         }
     }
 }
@@ -262,28 +312,39 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel
 //   MODE 2: out = (z0 + D) + cD*k; D_u <- out_u * gh (0 where NaN), the cell's
 //           term of z.gh, which subblock_sums reduces afterwards
 // (cu-G:1349-1427 in the order of cu-G:1885-1891).
+// The Jacobian comes from the cache jload when it is non-null, else it is
+// evaluated at ys; jstore (non-null only in the last stage) keeps the evaluated
+// one for the next backward step.
 template <int E, int TX, int TY, int NT, int MODE>
 __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, const double* __restrict__ src,
                                           double* __restrict__ dst, double* __restrict__ D,
                                           const double* __restrict__ z0g, const uint8_t* __restrict__ wc,
                                           const double* __restrict__ ys, long long off, double cZ, double cD,
-                                          double* __restrict__ out, const double* __restrict__ gh) {
+                                          double* __restrict__ out, const double* __restrict__ gh,
+                                          const double* __restrict__ jload, double* __restrict__ jstore) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
     constexpr int IN = TX * TY;
-#pragma unroll 1
+#pragma unroll kStageUnroll
     for (int q = threadIdx.x; q < N; q += NT) {
         const int r = HALO - E + q / W, c = HALO - E + q % W;
         const int s = r * RW + c;
         const long long o = off + (long long)r * g.ld + c;
+        const double a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
+        const int code = __ldg(wc + o);
         double ku, kv, kw;
         if (isnan(src[s])) {
             ku = kv = kw = kNaN;
         } else {
-            const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
-            adj_at<RW, RN>(P, src, s, __ldg(wc + o), J, ku, kv, kw);
+            JacT J;
+            if (jload) {
+                J = load_jac(jload, g.plane, o);
+            } else {
+                J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+                if (jstore) store_jac(jstore, g.plane, o, J);
+            }
+            adj_at<RW, RN>(P, src, s, code, J, ku, kv, kw);
         }
-        const double a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
         const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
@@ -316,12 +377,16 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
 // One backward RK4 step of the reference adjoint: stage 1 uses y(t_i) = yb,
 // stages 2-3 the midpoint yh, stage 4 y(t_{i-1}) = ya; the tile's 16x16
 // sub-block sums of z_u . gh (NaN terms skipped, cu-G:1457-1483) go to `row`.
+// Jacobian caches (null = evaluate): jb = J(y_i) left by the previous step's
+// last stage, jh = J(yh) from k_adj_mid; J(y_{i-1}) is evaluated in the last
+// stage and stored to ja for the next step.
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z,
                                                  double* __restrict__ zout, const double* __restrict__ yb,
                                                  const double* __restrict__ yh, const double* __restrict__ ya,
                                                  const uint8_t* __restrict__ wc, const double* __restrict__ gh,
-                                                 double* __restrict__ row, int nsbx) {
+                                                 double* __restrict__ row, int nsbx, const double* __restrict__ jb,
+                                                 const double* __restrict__ jh, double* __restrict__ ja) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -333,10 +398,10 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_step(DevMode
     load_region<RH, RW, NT>(A, z + off, g.ld, g.plane, vec_ok);
     __syncthreads();
     const double dt = P.dt;
-    adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh);
-    adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh);
-    adj_stage<1, TX, TY, NT, 1>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh);
-    adj_stage<0, TX, TY, NT, 2>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh);
+    adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb, nullptr);
+    adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
+    adj_stage<1, TX, TY, NT, 1>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
+    adj_stage<0, TX, TY, NT, 2>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, nullptr, ja);
     __syncthreads();
     subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
 }
@@ -362,7 +427,7 @@ __device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g,
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
     constexpr int IN = TX * TY;
-#pragma unroll 1
+#pragma unroll kStageUnroll
     for (int q = threadIdx.x; q < N; q += NT) {
         const int r = HALO - E + q / W, c = HALO - E + q % W;
         const int s = r * RW + c;
@@ -626,17 +691,18 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
 
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
-                           cudaStream_t st) {
+                           cudaStream_t st, const double* fin, double* fout, double* jh) {
     DISPATCH(tile, (k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, TY), NT, mid_smem<TX, TY>(), st>>>(
-                        P, g, ya, yb, gh, yh, Ea, Eb, E3, hw)));
+                        P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh)));
     return cudaGetLastError();
 }
 
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
-                            const double* gh, double* row, int nsbx, cudaStream_t st) {
+                            const double* gh, double* row, int nsbx, cudaStream_t st, const double* jb,
+                            const double* jh, double* ja) {
     DISPATCH(tile, (k_adj_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT), st>>>(
-                        P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx)));
+                        P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja)));
     return cudaGetLastError();
 }
 

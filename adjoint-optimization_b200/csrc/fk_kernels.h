@@ -36,10 +36,14 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
                              double* r1, double* r23, double* r4, int nsbx, cudaStream_t st);
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
-                           cudaStream_t st);
+                           cudaStream_t st, const double* fin = nullptr, double* fout = nullptr,
+                           double* jh = nullptr);
+// jb: cached J(y_i) (null = evaluate), jh: cached J(yh) (null = evaluate),
+// ja: where J(y_{i-1}) is stored for the next step (null = not kept).
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
-                            const double* gh, double* row, int nsbx, cudaStream_t st);
+                            const double* gh, double* row, int nsbx, cudaStream_t st, const double* jb = nullptr,
+                            const double* jh = nullptr, double* ja = nullptr);
 cudaError_t launch_dot_gh(const DevGrid& g, const double* z, const double* gh, double* row, int nsbx, int nsby,
                           cudaStream_t st);
 cudaError_t launch_sum_rows(const double* partial, int rows, int ntiles, double* out, cudaStream_t st);
