@@ -51,7 +51,9 @@ static DevModel make_model(const fkadj_params& p, double dt) {
 }
 
 // Hermite weights (cu-G:1217-1241 and the 27/64 of cu-G:1295-1298).
-static HermiteW make_hermite() {
+HermiteW hermite_weights();
+static HermiteW make_hermite() { return hermite_weights(); }
+HermiteW hermite_weights() {
     HermiteW w;
     double t = 1.0 / 3.0;
     w.c3[0] = (t - 1.0) * (t - 1.0) * (2.0 * t + 1.0);
@@ -391,7 +393,9 @@ fkadj_status Problem::forward(const double* Et, const double* y_ini, int nstep, 
     return FKADJ_OK;
 }
 
-fkadj_status Problem::run_objective(const double* yT, double* L0) {
+// Objective kernels at y(T), asynchronous: -L0 lands in osum_, z(T) (compact)
+// in zc_.
+fkadj_status Problem::objective_async(const double* yT) {
     if (!have_obj_) {
         set_error("problem has no objective");
         return FKADJ_ERR_ARG;
@@ -402,6 +406,12 @@ fkadj_status Problem::run_objective(const double* yT, double* L0) {
        "objective");
     CK(launch_sum_rows(opart_.as<double>(), 1, objective_blocks(n_num_), osum_.as<double>(), st_), "sum");
     launches_ += 3;
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::run_objective(const double* yT, double* L0) {
+    fkadj_status st0 = objective_async(yT);
+    if (st0) return st0;
     double s = 0;
     CK(cudaMemcpyAsync(&s, osum_.p, sizeof(double), cudaMemcpyDeviceToHost, st_), "download L0");
     CK(cudaStreamSynchronize(st_), "synchronize");

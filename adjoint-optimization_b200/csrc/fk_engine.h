@@ -54,7 +54,11 @@ struct TrajPlan {
     int seg_slots = 0;             // recompute buffer slots
 };
 
+class BatchEngine;
+
 class Problem {
+    friend class BatchEngine;
+
 public:
     ~Problem();
     fkadj_status init(const fkadj_params& p, double dt, int nt, const int* active_index, int nrows,
@@ -109,6 +113,7 @@ private:
     fkadj_status plan_trajectory(TrajPlan& tp);
     fkadj_status ensure_traj(const TrajPlan& tp);
     fkadj_status run_objective(const double* yT, double* L0);
+    fkadj_status objective_async(const double* yT);
     fkadj_status grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2);
     fkadj_status ensure_adjoint_work();
     fkadj_status download_grid(const double* d_state, double* host_dense);

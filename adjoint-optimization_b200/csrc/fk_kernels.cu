@@ -166,19 +166,21 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
     if (MODE != 2) __syncthreads();
 }
 
-// One RK4 step y -> y_out.  When `stages` is non-null the stage states
-// Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3 are stored there too
-// (three consecutive states), for the discrete-exact adjoint.
+// One RK4 step y -> y_out on tile (tbx, tby).  When `stages` is non-null the
+// stage states Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3 are stored
+// there too (three consecutive states), for the discrete-exact adjoint.
+// The tile functions may run several times per CTA (batched kernels): they
+// start by overwriting all the shared memory they read.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin,
-                                                 double* __restrict__ yout, const double* __restrict__ gh,
-                                                 double E0, double Eh, double E1, double* __restrict__ stages) {
+__device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ yin,
+                                              double* __restrict__ yout, const double* __restrict__ gh, double E0,
+                                              double Eh, double E1, double* __restrict__ stages, int tbx, int tby) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
     double* B = A + 3 * RN;
     double* D = B + 3 * RN;
-    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const int i0 = tby * TY, j0 = tbx * TX;
     // region origin: logical (i0 - HALO, j0 - HALO) = padded (i0, j0)
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
@@ -195,6 +197,13 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_fwd_step(DevMode
     fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3);
     fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4);
     fwd_stage<0, TX, TY, NT, 2>(P, B, A, D, y0g, ghs, g.ld, g.plane, E1, 0.0, dt * 1.0 / 6.0, yout + off, nullptr);
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+    k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin, double* __restrict__ yout,
+               const double* __restrict__ gh, double E0, double Eh, double E1, double* __restrict__ stages) {
+    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E0, Eh, E1, stages, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -230,19 +239,18 @@ __device__ __forceinline__ void store_jac(double* __restrict__ Jb, long long pla
 //   read from there instead of evaluated, and f(ya, Ea) goes to fout;
 //   J_F(yh)^T, used by stages 2 and 3 of the adjoint step, goes to jh.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya,
-                                                const double* __restrict__ yb,
-                                                const double* __restrict__ gh, double* __restrict__ yh,
-                                                double Ea, double Eb, double E3, HermiteW hw,
-                                                const double* __restrict__ fin, double* __restrict__ fout,
-                                                double* __restrict__ jh) {
+__device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ ya,
+                                             const double* __restrict__ yb, const double* __restrict__ gh,
+                                             double* __restrict__ yh, double Ea, double Eb, double E3,
+                                             const HermiteW& hw, const double* __restrict__ fin,
+                                             double* __restrict__ fout, double* __restrict__ jh, int tbx, int tby) {
     constexpr int H2 = 2;
     constexpr int RW = TX + 2 * H2, RH = TY + 2 * H2, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
     double* B = A + 3 * RN;
     double* C = B + 3 * RN;
-    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const int i0 = tby * TY, j0 = tbx * TX;
     // region origin: logical (i0 - 2, j0 - 2) = padded (i0 + 2, j0 + 2)
     const long long off = (long long)(i0 + HALO - H2) * g.ld + (j0 + HALO - H2);
     const bool vec_ok = ((g.ld | (j0 + HALO - H2)) & 1) == 0;
@@ -303,6 +311,14 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_mid(DevModel
             if (jh && !isnan(yv[0])) store_jac(jh, g.plane, o, fk_jacT(P, yv[0], yv[1], yv[2]));
         }
     }
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+    k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya, const double* __restrict__ yb,
+              const double* __restrict__ gh, double* __restrict__ yh, double Ea, double Eb, double E3, HermiteW hw,
+              const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh) {
+    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, blockIdx.x, blockIdx.y);
 }
 
 // One adjoint stage on the tile grown by E cells: k = L^T src + J_F(y)^T src,
@@ -381,18 +397,19 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
 // last stage, jh = J(yh) from k_adj_mid; J(y_{i-1}) is evaluated in the last
 // stage and stored to ja for the next step.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z,
-                                                 double* __restrict__ zout, const double* __restrict__ yb,
-                                                 const double* __restrict__ yh, const double* __restrict__ ya,
-                                                 const uint8_t* __restrict__ wc, const double* __restrict__ gh,
-                                                 double* __restrict__ row, int nsbx, const double* __restrict__ jb,
-                                                 const double* __restrict__ jh, double* __restrict__ ja) {
+__device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ z,
+                                              double* __restrict__ zout, const double* __restrict__ yb,
+                                              const double* __restrict__ yh, const double* __restrict__ ya,
+                                              const uint8_t* __restrict__ wc, const double* __restrict__ gh,
+                                              double* __restrict__ row, int nsbx, const double* __restrict__ jb,
+                                              const double* __restrict__ jh, double* __restrict__ ja, int tbx,
+                                              int tby) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
     double* B = A + 3 * RN;
     double* D = B + 3 * RN;
-    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
     load_region<RH, RW, NT>(A, z + off, g.ld, g.plane, vec_ok);
@@ -404,6 +421,15 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_step(DevMode
     adj_stage<0, TX, TY, NT, 2>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, nullptr, ja);
     __syncthreads();
     subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+    k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z, double* __restrict__ zout,
+               const double* __restrict__ yb, const double* __restrict__ yh, const double* __restrict__ ya,
+               const uint8_t* __restrict__ wc, const double* __restrict__ gh, double* __restrict__ row, int nsbx,
+               const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja) {
+    adj_step_tile<TX, TY, NT>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------ exact-mode adjoint
@@ -472,12 +498,12 @@ __device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g,
 // Y4 of step s (three consecutive states, written by k_fwd_step).
 // 16x16 sub-block sums: r1 <- b.a1, r23 <- b.(a2 + a3), r4 <- b.a4.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_exact(DevModel P, DevGrid g, const double* __restrict__ lam,
-                                                  double* __restrict__ lamout, const double* __restrict__ y,
-                                                  const double* __restrict__ stages,
-                                                  const uint8_t* __restrict__ wc, const double* __restrict__ gh,
-                                                  double* __restrict__ r1, double* __restrict__ r23,
-                                                  double* __restrict__ r4, int nsbx) {
+__device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ lam,
+                                               double* __restrict__ lamout, const double* __restrict__ y,
+                                               const double* __restrict__ stages, const uint8_t* __restrict__ wc,
+                                               const double* __restrict__ gh, double* __restrict__ r1,
+                                               double* __restrict__ r23, double* __restrict__ r4, int nsbx, int tbx,
+                                               int tby) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int IN = TX * TY;
     extern __shared__ double4 smem_raw[];
@@ -485,7 +511,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_exact(DevMod
     double* B = A + 3 * RN;
     double* D = B + 3 * RN;
     double* T3 = D + 3 * IN;  // a3_u on the tile
-    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
     load_region<RH, RW, NT>(A, lam + off, g.ld, g.plane, vec_ok);
@@ -514,6 +540,75 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT)) k_adj_exact(DevMod
             return z0(c6 * __ldg(lam + off + (long long)(r + HALO) * g.ld + (c + HALO)) * ghv(r, c));
         },
         r4, i0, j0, nsbx);
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+    k_adj_exact(DevModel P, DevGrid g, const double* __restrict__ lam, double* __restrict__ lamout,
+                const double* __restrict__ y, const double* __restrict__ stages, const uint8_t* __restrict__ wc,
+                const double* __restrict__ gh, double* __restrict__ r1, double* __restrict__ r23,
+                double* __restrict__ r4, int nsbx) {
+    adj_exact_tile<TX, TY, NT>(P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx, blockIdx.x, blockIdx.y);
+}
+
+// ---------------------------------------------------------------- batched
+//
+// One launch per kernel kind and tick runs the tiles of every instance that
+// has that kind of work this tick.  The tick's work queue is passed by value
+// (no per-tick copies, so a tick is a plain launch that a CUDA graph can
+// hold); a persistent grid of CTAs strides over the queue's tiles, each item
+// owning a contiguous range of tile indices.
+template <int TX, int TY, int NT>
+__device__ __forceinline__ int find_item(const BatchTick& t, int tile) {
+    int lo = 0, hi = t.n - 1;
+    while (lo < hi) {  // last item whose first tile is <= tile
+        const int mid = (lo + hi + 1) >> 1;
+        if (t.item[mid].tile0 <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+    k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchTick t) {
+    for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
+        const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
+        const BatchInstance& I = inst[it.inst];
+        const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
+        __syncthreads();
+        fwd_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, I.gh, it.E0, it.E1, it.E2, it.stages, tbx, tby);
+    }
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+    k_batch_mid(const BatchInstance* __restrict__ inst, const BatchTick t, HermiteW hw) {
+    for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
+        const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
+        const BatchInstance& I = inst[it.inst];
+        const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
+        __syncthreads();
+        adj_mid_tile<TX, TY, NT>(I.P, I.g, it.a, it.b, I.gh, it.out, it.E0, it.E1, it.E2, hw, it.fin, it.fout,
+                                 it.jh, tbx, tby);
+    }
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+    k_batch_adj(const BatchInstance* __restrict__ inst, const BatchTick t) {
+    for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
+        const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
+        const BatchInstance& I = inst[it.inst];
+        const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
+        __syncthreads();
+        if (it.kind == BATCH_ADJ_EXACT)
+            adj_exact_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, it.b, it.stages, I.wc, I.gh, it.row, it.row2,
+                                       it.row3, I.nsbx, tbx, tby);
+        else
+            adj_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, it.b, it.c, it.d, I.wc, I.gh, it.row, I.nsbx, it.jb,
+                                      it.jh, it.ja, tbx, tby);
+    }
 }
 
 // z_u . gh per 16x16 sub-block (NaN terms skipped), one warp per sub-block,
@@ -624,8 +719,33 @@ static cudaError_t setup_tile() {
     if ((e = cudaFuncSetAttribute(k_adj_exact<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)exact_smem<TX, TY>())))
         return e;
+    if ((e = cudaFuncSetAttribute(k_batch_fwd<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s))) return e;
+    if ((e = cudaFuncSetAttribute(k_batch_mid<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)mid_smem<TX, TY>())))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_batch_adj<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)exact_smem<TX, TY>())))
+        return e;
     return cudaFuncSetAttribute(k_adj_mid<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)mid_smem<TX, TY>());
+}
+
+// Persistent grid for a batched launch: as many CTAs as fit on the device at
+// once (occupancy x SMs), never more than the tick's tiles.
+template <class K>
+static int persistent_grid(K kernel, int nt, size_t smem, int tiles) {
+    static thread_local int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int g = sms * per_sm;
+    return tiles < g ? tiles : g;
 }
 
 // Tile presets (TX, TY, threads).  All TY divide 64 (the row padding of the
@@ -659,14 +779,14 @@ cudaError_t kernels_init() {
     return cudaSuccess;
 }
 
-#define DISPATCH(tile, CALL)                              \
+#define DISPATCH(tile, ...)                               \
     switch (tile) {                                       \
-        case 1: { constexpr int TX = 32, TY = 32, NT = 512; CALL; } break; \
-        case 2: { constexpr int TX = 64, TY = 32, NT = 512; CALL; } break; \
-        case 3: { constexpr int TX = 32, TY = 16, NT = 256; CALL; } break; \
-        case 4: { constexpr int TX = 16, TY = 16, NT = 256; CALL; } break; \
-        case 5: { constexpr int TX = 64, TY = 16, NT = 512; CALL; } break; \
-        default: { constexpr int TX = 32, TY = 32, NT = 256; CALL; } break; \
+        case 1: { constexpr int TX = 32, TY = 32, NT = 512; __VA_ARGS__; } break; \
+        case 2: { constexpr int TX = 64, TY = 32, NT = 512; __VA_ARGS__; } break; \
+        case 3: { constexpr int TX = 32, TY = 16, NT = 256; __VA_ARGS__; } break; \
+        case 4: { constexpr int TX = 16, TY = 16, NT = 256; __VA_ARGS__; } break; \
+        case 5: { constexpr int TX = 64, TY = 16, NT = 512; __VA_ARGS__; } break; \
+        default: { constexpr int TX = 32, TY = 32, NT = 256; __VA_ARGS__; } break; \
     }
 
 static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
@@ -703,6 +823,37 @@ cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const
                             const double* jh, double* ja) {
     DISPATCH(tile, (k_adj_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT), st>>>(
                         P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st) {
+    if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
+    DISPATCH(tile, {
+        const size_t sm = stencil_smem<TX, TY>(NT);
+        const int grid = persistent_grid(k_batch_fwd<TX, TY, NT>, NT, sm, t.tiles);
+        k_batch_fwd<TX, TY, NT><<<grid, NT, sm, st>>>(d_inst, t);
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchTick& t, const HermiteW& hw,
+                             cudaStream_t st) {
+    if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
+    DISPATCH(tile, {
+        const size_t sm = mid_smem<TX, TY>();
+        const int grid = persistent_grid(k_batch_mid<TX, TY, NT>, NT, sm, t.tiles);
+        k_batch_mid<TX, TY, NT><<<grid, NT, sm, st>>>(d_inst, t, hw);
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st) {
+    if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
+    DISPATCH(tile, {
+        const size_t sm = exact_smem<TX, TY>();
+        const int grid = persistent_grid(k_batch_adj<TX, TY, NT>, NT, sm, t.tiles);
+        k_batch_adj<TX, TY, NT><<<grid, NT, sm, st>>>(d_inst, t);
+    });
     return cudaGetLastError();
 }
 

@@ -19,6 +19,51 @@ struct HermiteW {
     double c2;     // weight of dt*f(y3) in the quartic
 };
 
+// ------------------------------------------------------------ batched ticks
+// Per-instance constants of a batch (device array).
+struct BatchInstance {
+    DevModel P;
+    DevGrid g;
+    const double* gh;
+    const uint8_t* wc;
+    int nsbx;
+};
+
+enum BatchKind { BATCH_FWD = 0, BATCH_MID = 1, BATCH_ADJ_REF = 2, BATCH_ADJ_EXACT = 3 };
+
+// One instance's work of one kind in one tick; it owns tiles
+// [tile0, tile0 + ntx*nty) of the tick's launch.  Field use by kind:
+//   FWD        a = y_in, out = y_out, stages (or null), E0/E1/E2 = Et[i], Eh[i], Et[i+1]
+//   MID        a = y_{i-1}, b = y_i, out = yh, E0/E1/E2 = Et[i-1], Et[i], E(t_{i-1}+dt/3),
+//              fin/fout (f carry), jh (J(yh) out)
+//   ADJ_REF    a = z, out = z_out, b = y_i, c = yh, d = y_{i-1}, row, jb/jh/ja (J caches)
+//   ADJ_EXACT  a = lambda, out = lambda_out, b = y_s, stages, row/row2/row3
+struct BatchItem {
+    int inst, tile0, ntx, kind;
+    const double *a, *b, *c, *d;
+    double *out, *stages;
+    double E0, E1, E2;
+    const double* fin;
+    double *fout, *jh;
+    const double* jb;
+    double* ja;
+    double *row, *row2, *row3;
+};
+
+constexpr int kBatchMaxItems = 128;
+
+// A tick's work queue for one kernel kind, passed to the launch by value.
+struct BatchTick {
+    int n;      // items
+    int tiles;  // total tiles
+    BatchItem item[kBatchMaxItems];
+};
+
+cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st);
+cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchTick& t, const HermiteW& hw,
+                             cudaStream_t st);
+cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st);
+
 int tile_count();
 TileShape tile_shape(int tile);
 int tiles_of(int tile, const DevGrid& g);

@@ -158,6 +158,44 @@ void fkadj_problem_set_profiling(fkadj_problem *pb, int enable);
 void fkadj_problem_kernel_time(const fkadj_problem *pb, int kernel, double *avg_ms, int64_t *samples);
 
 /* ------------------------------------------------------------------------
+ * Batches: many independent problems (different grids, horizons, pulses,
+ * obstacle layouts) advanced together.  Every tick takes the next step of
+ * every running job and runs them as at most three launches of persistent
+ * kernels over a work queue of (problem, tile) items.  No reference
+ * counterpart (the reference runs one instance per MATLAB call,
+ * src/cuda/simple_grad_desc.m:82).  Problems of a batch live on the batch's
+ * stream; one job per problem runs at a time; at most 128 jobs run at once.
+ * --------------------------------------------------------------------- */
+typedef struct fkadj_batch fkadj_batch;
+
+fkadj_status fkadj_batch_create(fkadj_batch **out, const fkadj_options *opt);
+void fkadj_batch_destroy(fkadj_batch *b);
+/* Adds a resident problem (geometry, objective); grad_mode / ckpt_policy /
+ * ckpt_budget_bytes as in fkadj_options.  S may be NULL for forward-only. */
+fkadj_status fkadj_batch_add_problem(fkadj_batch *b, const fkadj_params *p, double dt, int nt,
+                                     const int *active_index, int nrows, int ncols, int n_num,
+                                     const double *gh_num, const double *gamma, int64_t S_ncol,
+                                     const int64_t *S_colptr, const int64_t *S_rowidx, const double *S_val,
+                                     double alpha, int grad_mode, int ckpt_policy, int64_t ckpt_budget_bytes,
+                                     int *problem_id);
+fkadj_status fkadj_batch_remove_problem(fkadj_batch *b, int problem_id);
+/* Queues an objective (want_grad = 0) or objective + gradient job; y_ini may be
+ * NULL to re-use the problem's resident initial state. */
+fkadj_status fkadj_batch_submit(fkadj_batch *b, int problem_id, const double *Et, const double *y_ini,
+                                int want_grad, int *job_id);
+/* One tick (*active receives the number of unfinished jobs), or ticks until
+ * every job is done. */
+fkadj_status fkadj_batch_tick(fkadj_batch *b, int *active);
+fkadj_status fkadj_batch_run(fkadj_batch *b);
+int fkadj_batch_job_done(const fkadj_batch *b, int job_id);
+/* Results of a finished job: gradE receives min(n_gradE, nt+1) values. */
+fkadj_status fkadj_batch_result(fkadj_batch *b, int job_id, double *L0, double *LE, double *Lcost,
+                                double *gradE, int64_t n_gradE);
+fkadj_status fkadj_batch_release(fkadj_batch *b, int job_id);
+/* out[0] kernel launches, out[1] ticks, out[2] device bytes held. */
+void fkadj_batch_stats(const fkadj_batch *b, int64_t out[3]);
+
+/* ------------------------------------------------------------------------
  * z.gh without allocating.  No counterpart in the reference: it is the
  * reduction the reference takes once per backward step (sum of z_u * gh over
  * the grid, NaN terms skipped), offered to callers that cannot call
