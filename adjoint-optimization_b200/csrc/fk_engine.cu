@@ -242,6 +242,25 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     return FKADJ_OK;
 }
 
+int64_t Problem::estimate_bytes(int nrows, int ncols, int nt, int n_num, int64_t nnz, int grad_mode, int policy,
+                                bool want_grad) {
+    const int64_t ld = round_up(round_up(ncols, 64) + 2 * HALO, 8);
+    const int64_t rows = round_up(nrows, 64) + 2 * HALO;
+    const int64_t plane = rows * ld * 8, state = 3 * plane;
+    int64_t b = plane + plane / 8 + (int64_t)n_num * (8 + 48) + nnz * 12 + 4 * state;  // geometry, compact, work
+    if (!want_grad) return b;
+    const int64_t nsb = (round_up(ncols, 64) / 16) * (round_up(nrows, 64) / 16);
+    b += 2 * state + (int64_t)(3 * nt + 1) * (nsb + 1) * 8;  // adjoint pair, partials
+    b += grad_mode == FKADJ_GRAD_EXACT ? 3 * state : state + 27 * plane;  // stages | yh + caches
+    if (policy == FKADJ_CKPT_FULL) {
+        b += (int64_t)(nt + 1) * state;
+    } else {
+        const int64_t c = std::max(2, (int)std::ceil(std::sqrt((double)nt)));
+        b += ((nt + c - 1) / c + 1 + c - 1) * state;
+    }
+    return b;
+}
+
 int64_t Problem::device_bytes() const {
     const DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_,
                            &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &y0res_, &stg_, &jcache_, &fcache_};

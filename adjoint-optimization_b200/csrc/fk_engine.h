@@ -73,6 +73,11 @@ public:
                       double* gradE, double* yf);
 
     int64_t device_bytes() const;
+    // Device bytes a problem of this size will hold once a job has run
+    // (geometry, work states, adjoint work, Jacobian caches, trajectory store
+    // under `policy`), for admission control before anything is allocated.
+    static int64_t estimate_bytes(int nrows, int ncols, int nt, int n_num, int64_t nnz, int grad_mode,
+                                  int policy, bool want_grad);
     Timing last_timing() const { return timing_; }
     int64_t last_launches() const { return launches_; }
 

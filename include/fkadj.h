@@ -196,6 +196,38 @@ fkadj_status fkadj_batch_release(fkadj_batch *b, int job_id);
 void fkadj_batch_stats(const fkadj_batch *b, int64_t out[3]);
 
 /* ------------------------------------------------------------------------
+ * Serving: a worker thread owns the GPU and runs a batch continuously.
+ * Requests (any thread) queue in arrival order and are admitted between ticks
+ * while their estimated device footprint fits hbm_budget_bytes (0 = 80% of
+ * free memory) and fewer than 128 run; admitted requests share every launch
+ * with the running ones and free their memory when they finish.  All waits are
+ * bounded.  No reference counterpart.  options.grad_mode / ckpt_policy apply
+ * to every request (ckpt_policy FULL or else sqrt checkpoints).
+ * --------------------------------------------------------------------- */
+typedef struct fkadj_server fkadj_server;
+
+fkadj_status fkadj_server_create(fkadj_server **out, const fkadj_options *opt, int64_t hbm_budget_bytes);
+/* Finishes the queued and running requests, then stops the worker. */
+void fkadj_server_destroy(fkadj_server *s);
+/* Copies the request; returns at once with its id. */
+fkadj_status fkadj_server_submit(fkadj_server *s, const fkadj_params *p, double dt, int nt,
+                                 const int *active_index, int nrows, int ncols, int n_num,
+                                 const double *gh_num, const double *gamma, int64_t S_ncol,
+                                 const int64_t *S_colptr, const int64_t *S_rowidx, const double *S_val,
+                                 double alpha, const double *Et, const double *y_ini, int want_grad,
+                                 int64_t *request_id);
+/* 1 done, 0 queued or running, -2 failed, -1 unknown id. */
+int fkadj_server_poll(fkadj_server *s, int64_t request_id);
+/* Waits at most timeout_s seconds (FKADJ_ERR_TIMEOUT when it expires). */
+fkadj_status fkadj_server_wait(fkadj_server *s, int64_t request_id, double timeout_s);
+/* Results of a finished request, then forgets it.  latency_s[0] = submit to
+ * done, latency_s[1] = submit to admission (may be NULL). */
+fkadj_status fkadj_server_result(fkadj_server *s, int64_t request_id, double *L0, double *LE, double *Lcost,
+                                 double *gradE, int64_t n_gradE, double latency_s[2]);
+/* out: completed, failed, queued, running, peak running, device bytes reserved. */
+void fkadj_server_stats(fkadj_server *s, int64_t out[6]);
+
+/* ------------------------------------------------------------------------
  * z.gh without allocating.  No counterpart in the reference: it is the
  * reduction the reference takes once per backward step (sum of z_u * gh over
  * the grid, NaN terms skipped), offered to callers that cannot call

@@ -1,0 +1,87 @@
+"""Serving (fkadj_server_*): requests of different sizes arriving while others
+run are admitted and computed together; each result equals the one-shot
+result and is the same alone and in the mix; waits are bounded."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from fkadj import _lib, api, workloads as W
+from fkadj.serve import Server
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(seed):
+    specs = [(64, 80, 200, True), (48, 48, 120, False), (96, 64, 90, True), (32, 128, 300, True),
+             (80, 80, 60, False), (64, 64, 150, True)]
+    return [(W.make_instance(nr, nt, seed=seed + k, ncols=nc, n_obstacles=5, intervals=10,
+                             objective="gradient" if k % 2 else "mean_u2", alpha=0.1), g)
+            for k, (nr, nc, nt, g) in enumerate(specs)]
+
+
+def test_served_results_match_one_shot_and_are_mix_invariant():
+    reqs = _requests(300)
+    target, _ = reqs[0]
+    with Server() as srv:
+        rid = srv.submit(target)
+        assert srv.wait(rid, 120)
+        alone = srv.result(rid)
+    with Server() as srv:
+        ids = []
+        # staggered arrivals from another thread while earlier requests run
+        def client():
+            for inst, g in reqs[1:]:
+                ids.append((srv.submit(inst, want_grad=g), inst, g))
+                time.sleep(0.002)
+        th = threading.Thread(target=client)
+        th.start()
+        time.sleep(0.001)
+        rid = srv.submit(target)
+        th.join()
+        assert srv.wait(rid, 120)
+        mixed = srv.result(rid)
+        results = []
+        for r, inst, g in ids:
+            assert srv.wait(r, 120)
+            results.append((srv.result(r), inst, g))
+        st = srv.stats
+        assert st["failed"] == 0 and st["completed"] == len(reqs)
+    assert np.array_equal(alone["gradE"], mixed["gradE"]) and alone["Lcost"] == mixed["Lcost"]
+    for res, inst, g in results:
+        if g:
+            ref = api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                                 inst.ghost, inst.gamma, inst.S, inst.alpha, params=inst.params)
+            assert np.linalg.norm(res["gradE"] - ref[0]) <= 1e-12 * np.linalg.norm(ref[0])
+            assert abs(res["Lcost"] - ref[1]) <= 1e-12 * abs(ref[1])
+        else:
+            ref = api.Problem(inst).objective(inst.Et, inst.y0)
+            assert abs(res["Lcost"] - ref["Lcost"]) <= 1e-12 * abs(ref["Lcost"])
+        assert res["latency_s"] >= res["queue_s"] >= 0
+
+
+def test_admission_respects_the_hbm_budget():
+    reqs = _requests(400)
+    # a budget that fits about two of these requests at a time
+    with Server(hbm_budget_bytes=25_000_000) as srv:
+        ids = [srv.submit(inst, want_grad=g) for inst, g in reqs]
+        for r in ids:
+            assert srv.wait(r, 120)
+        st = srv.stats
+        assert st["completed"] == len(reqs)
+        assert st["peak_running"] < len(reqs)
+        for r in ids:
+            srv.result(r)
+
+
+def test_wait_is_bounded():
+    inst = W.make_instance(128, 3000, seed=9, n_obstacles=5)
+    with Server() as srv:
+        rid = srv.submit(inst)
+        t0 = time.perf_counter()
+        done = srv.wait(rid, 1e-4)
+        assert time.perf_counter() - t0 < 5.0
+        assert done in (True, False)
+        assert srv.wait(rid, 120)
+        srv.result(rid)
