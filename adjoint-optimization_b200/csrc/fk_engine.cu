@@ -483,19 +483,30 @@ fkadj_status Problem::objective(const double* Et, const double* y_ini, double* L
 
 fkadj_status Problem::plan_trajectory(TrajPlan& tp) {
     const double sb = (double)state_bytes();
+    const int c = std::max(2, (int)std::ceil(std::sqrt((double)nt_)));
+    const int sqrt_slots = (nt_ + c - 1) / c + 1 + (c - 1);
     int pol = ckpt_policy_;
-    if (pol == FKADJ_CKPT_AUTO) pol = ((double)(nt_ + 1) * sb <= (double)ckpt_budget_) ? FKADJ_CKPT_FULL : FKADJ_CKPT_SQRT;
-    if (pol == FKADJ_CKPT_BINOMIAL) pol = FKADJ_CKPT_SQRT;
+    if (pol == FKADJ_CKPT_AUTO) {
+        if ((double)(nt_ + 1) * sb <= (double)ckpt_budget_) pol = FKADJ_CKPT_FULL;
+        else if ((double)sqrt_slots * sb <= (double)ckpt_budget_) pol = FKADJ_CKPT_SQRT;
+        else pol = FKADJ_CKPT_BINOMIAL;
+    }
     tp.policy = pol;
     if (pol == FKADJ_CKPT_FULL) {
         tp.stride = 1;
         tp.nslots = nt_ + 1;
         tp.seg_slots = 0;
-    } else {
-        const int c = std::max(2, (int)std::ceil(std::sqrt((double)nt_)));
+    } else if (pol == FKADJ_CKPT_SQRT) {
         tp.stride = c;
         tp.nslots = (nt_ + c - 1) / c + 1;
         tp.seg_slots = c - 1;
+    } else {
+        // binomial: y_0, y_nt and s free snapshots within the budget, plus one
+        // scratch state for replays when no snapshot is free
+        const int64_t fit = (int64_t)((double)ckpt_budget_ / sb) - 1;
+        tp.stride = 0;
+        tp.nslots = (int)std::max<int64_t>(2, std::min<int64_t>(fit, nt_ + 1));
+        tp.seg_slots = 1;
     }
     const double need = (double)(tp.nslots + tp.seg_slots) * sb;
     if (ckpt_policy_ != FKADJ_CKPT_FULL && need > (double)ckpt_budget_) {
@@ -614,6 +625,62 @@ fkadj_status Problem::autotune() {
     return FKADJ_OK;
 }
 
+// C(n, k) for small k, saturating at 2^62.
+static int64_t binom_small_k(int64_t n, int k) {
+    long double r = 1.0L;
+    for (int i = 1; i <= k; ++i) {
+        r = r * (long double)(n - k + i) / (long double)i;
+        if (r > 4.0e18L) return (int64_t)1 << 62;
+    }
+    return (int64_t)(r + 0.5L);
+}
+
+fkadj_status Problem::advance(int a, int m, const double* src, double* dst) {
+    fkadj_status s;
+    const double* cur = src;
+    double* s1 = state_buf(1);
+    double* s2 = state_buf(2);
+    for (int t = a; t < m; ++t) {
+        double* out = (t == m - 1) ? dst : ((cur == s1) ? s2 : s1);
+        if ((s = step_forward(t, cur, out))) return s;
+        cur = out;
+    }
+    return FKADJ_OK;
+}
+
+// Binomial (revolve) reversal of steps [a, b): visits j = b-1, ..., a in
+// that order, each with y_j, using the snapshot slots in `free` and
+// recomputing forward from y_a.  With s free slots and t = b - a steps, r is
+// the least number of sweeps with C(s + r, s) >= t (Griewank's binomial
+// bound); the checkpoint goes where the right part holds C(s - 1 + r, s - 1)
+// steps, which it can reverse with one slot fewer, and the left part holds at
+// most C(s + r - 1, s) steps, which it can reverse in one sweep fewer.
+fkadj_status Problem::reverse_binomial(int a, int b, double* ya, std::vector<double*>& free,
+                                       const std::function<fkadj_status(int, const double*)>& visit) {
+    fkadj_status s;
+    if (b - a == 1) return visit(a, ya);
+    const int ns = (int)free.size();
+    if (ns == 0) {  // no snapshot left: replay from y_a for every state
+        double* scr = segslot(0);
+        for (int j = b - 1; j > a; --j) {
+            if ((s = advance(a, j, ya, scr))) return s;
+            if ((s = visit(j, scr))) return s;
+        }
+        return visit(a, ya);
+    }
+    const int64_t t = b - a;
+    int r = 1;
+    while (binom_small_k(ns + r, r) < t) ++r;
+    const int64_t right = std::min<int64_t>(binom_small_k(ns - 1 + r, r), t - 1);
+    const int m = b - (int)right;
+    double* sm = free.back();
+    free.pop_back();
+    if ((s = advance(a, m, ya, sm))) return s;
+    if ((s = reverse_binomial(m, b, sm, free, visit))) return s;
+    free.push_back(sm);
+    return reverse_binomial(a, m, ya, free, visit);
+}
+
 // Discrete-exact backward sweep: per step s (last to first) the forward step
 // from y_s is replayed once to store its stage states, then k_adj_exact maps
 // lambda_{s+1} -> lambda_s and leaves the three E-sensitivity partials.
@@ -646,6 +713,12 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
         for (int t = nt - 1; t >= 0; --t)
             if ((s = back(t, slot(t)))) return s;
         return FKADJ_OK;
+    }
+    if (tp.policy == FKADJ_CKPT_BINOMIAL) {
+        std::vector<double*> free;
+        for (int k = tp.nslots - 1; k >= 2; --k) free.push_back(slot(k));
+        return reverse_binomial(0, nt, slot(0), free,
+                                [&](int t, const double* y) { return back(t, y); });
     }
     for (int k = K - 1; k >= 0; --k) {
         const int s0 = k * c, s1 = std::min(s0 + c, nt);
@@ -689,9 +762,11 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         tuned_ = tuned_fwd_ = true;
     }
     double* cur = slot(0);
+    const bool binomial = tp.policy == FKADJ_CKPT_BINOMIAL;
     for (int i = 0; i < nt; ++i) {
         double* out;
         if (tp.policy == FKADJ_CKPT_FULL) out = slot(i + 1);
+        else if (binomial) out = (i + 1 == nt) ? slot(1) : ((cur == state_buf(1)) ? state_buf(2) : state_buf(1));
         else if ((i + 1) % c == 0) out = slot((i + 1) / c);
         else if (i + 1 == nt) out = slot(K);
         else out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
@@ -747,6 +822,21 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     };
     if (exact) {
         // backward sweep done above
+    } else if (binomial) {
+        // visits j = nt-1 .. 0 in order; step i = j+1 needs y_j and y_{j+1}:
+        // y_{j+1} is the previous visit's state, kept in state_buf(0)
+        std::vector<double*> free;
+        for (int k = tp.nslots - 1; k >= 2; --k) free.push_back(slot(k));
+        const double* prev = slot(1);  // y(T)
+        double* keep = state_buf(0);
+        auto visit = [&](int j, const double* yj) -> fkadj_status {
+            fkadj_status r = back_step(j + 1, yj, prev);
+            if (r) return r;
+            CK(cudaMemcpyAsync(keep, yj, state_bytes(), cudaMemcpyDeviceToDevice, st_), "keep state");
+            prev = keep;
+            return FKADJ_OK;
+        };
+        if ((s = reverse_binomial(0, nt, slot(0), free, visit))) return s;
     } else if (tp.policy == FKADJ_CKPT_FULL) {
         for (int i = nt; i > 0; --i)
             if ((s = back_step(i, slot(i - 1), slot(i)))) return s;

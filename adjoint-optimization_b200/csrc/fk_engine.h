@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -120,6 +121,9 @@ private:
     fkadj_status run_objective(const double* yT, double* L0);
     fkadj_status objective_async(const double* yT);
     fkadj_status grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2);
+    fkadj_status advance(int a, int m, const double* src, double* dst);
+    fkadj_status reverse_binomial(int a, int b, double* ya, std::vector<double*>& free,
+                                  const std::function<fkadj_status(int, const double*)>& visit);
     fkadj_status ensure_adjoint_work();
     fkadj_status download_grid(const double* d_state, double* host_dense);
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }

@@ -166,3 +166,27 @@ def test_exact_gradient_central_fd_on_intervals():
             Jm = pb.objective(W.piecewise_constant(inst.nt, Am)[0], inst.y0)["Lcost"]
             fd = (Jp - Jm) / (2 * h)
             assert abs(fd - dJdA[k]) <= 1e-6 * np.abs(dJdA).max() + 1e-5 * abs(fd), (k, fd, dJdA[k])
+
+
+def _state_bytes(nrows, ncols):
+    rows = (nrows + 63) // 64 * 64 + 8
+    ld = ((ncols + 63) // 64 * 64 + 8 + 7) // 8 * 8
+    return 3 * rows * ld * 8
+
+
+@pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
+@pytest.mark.parametrize("slots", [2, 4, 9])
+def test_binomial_checkpointing_equals_full_storage(mode, slots):
+    """Binomial reversal with a budget of `slots` states (2 = no free snapshot,
+    every state replayed from y_0) gives the same bits as full storage."""
+    inst = _inst(48, 70 if slots == 2 else 130, seed=23, ncols=64, objective="gradient")
+    args = (inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows, inst.ghost,
+            inst.gamma, inst.S, 0.2)
+    full = api.fk_grad_Et(*args, params=inst.params,
+                          opts=api.options(grad_mode=mode, ckpt_policy=_lib.CKPT_FULL))
+    budget = (slots + 1) * _state_bytes(inst.nrows, inst.ncols)
+    bino = api.fk_grad_Et(*args, params=inst.params,
+                          opts=api.options(grad_mode=mode, ckpt_policy=_lib.CKPT_BINOMIAL,
+                                           ckpt_budget_bytes=budget))
+    assert np.array_equal(full[0], bino[0])
+    assert full[1] == bino[1]
