@@ -54,6 +54,7 @@ fkadj_status BatchEngine::init(const fkadj_options* opt) {
     }
     const int t = (opt_.tile > 0 && opt_.tile <= tile_count()) ? opt_.tile - 1 : 0;
     tiles_[0] = tiles_[1] = tiles_[2] = t;
+    tuned_ = opt_.tile > 0 && opt_.tile <= tile_count();
     hw_ = hermite_weights();
     BCK(cudaMallocHost(&t_fwd_, sizeof(BatchTick)), "pinned tick");
     BCK(cudaMallocHost(&t_mid_, sizeof(BatchTick)), "pinned tick");
@@ -196,6 +197,11 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
     j->Et.assign(Et, Et + P.nt_ + 1);
     if (want_grad) {
         if ((s = P.plan_trajectory(j->tp))) return s;
+        if (j->tp.policy == FKADJ_CKPT_BINOMIAL) {
+            set_error("batched jobs store full or sqrt trajectories; the binomial schedule runs in the "
+                      "standalone engine (raise ckpt_budget_bytes or use fkadj_problem_grad)");
+            return FKADJ_ERR_NOMEM;
+        }
         if ((s = P.ensure_traj(j->tp))) return s;
         if ((s = P.ensure_adjoint_work())) return s;
         if ((s = P.upload_state(y_ini, P.slot(0)))) return s;
@@ -413,6 +419,27 @@ fkadj_status BatchEngine::finish_poll(Job& j) {
 fkadj_status BatchEngine::tick(int* active) {
     fkadj_status s;
     if (inst_dirty_ && (s = sync_instances())) return s;
+    if (!tuned_ && !active_.empty()) {
+        // tile presets: the standalone autotuner's choice on the largest job
+        int best = -1;
+        int64_t cells = -1;
+        for (int id : active_) {
+            Problem& P = *probs_[jobs_[id]->prob];
+            const int64_t c = (int64_t)P.g_.nrows * P.g_.ncols;
+            if (jobs_[id]->want_grad && c > cells) cells = c, best = jobs_[id]->prob;
+        }
+        if (best >= 0) {
+            Problem& P = *probs_[best];
+            const bool keep = P.autotune_;
+            P.autotune_ = true;
+            if ((s = P.autotune())) return s;
+            P.autotune_ = keep;
+            tiles_[0] = P.tk_[Problem::T_FWD];
+            tiles_[1] = P.tk_[Problem::T_MID];
+            tiles_[2] = P.grad_mode_ == FKADJ_GRAD_EXACT ? P.tk_[Problem::T_EXACT] : P.tk_[Problem::T_ADJ];
+            tuned_ = true;
+        }
+    }
     t_fwd_->n = t_fwd_->tiles = 0;
     t_mid_->n = t_mid_->tiles = 0;
     t_adj_->n = t_adj_->tiles = 0;

@@ -93,6 +93,7 @@ private:
     cudaStream_t st_ = nullptr;
     bool own_stream_ = false;
     int tiles_[3] = {0, 0, 0};  // fwd, mid, adj presets
+    bool tuned_ = false;        // presets fixed (options.tile > 0) or autotuned
     HermiteW hw_{};
     std::vector<std::unique_ptr<Problem>> probs_;
     std::vector<BatchInstance> inst_host_;

@@ -1,0 +1,157 @@
+"""Workload measurements beyond the headline bench line (one JSON line each).
+
+  python -m fkadj.suite ckpt   [--n 512 --nt 20000]
+      one 512^2 x 20000-step gradient under FULL storage, sqrt checkpoints and
+      a binomial schedule within a small budget (device time per gradient)
+  python -m fkadj.suite batch  [--count 64 --max-side 1024 --nt-scale 1]
+      uneven instances (sides {128..1024}, horizons U{1000..20000} x nt-scale,
+      hole density 3e-4, 100-400 intervals): one resident problem at a time vs
+      all of them in one batch; gradients/s and makespan
+  python -m fkadj.suite serve  [--rates 10,50,200,500 --requests 48 ...]
+      Poisson arrivals, half objective-only, half objective+gradient, sizes as
+      above: served latency p50/p99 and throughput, against the same stream
+      solved one request at a time (FIFO, each request's standalone time)
+
+Sizes can be scaled down (max side, horizon scale) to fit a time budget; the
+line says which.  Inputs are seeded synthetic instances (fkadj.workloads).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import _lib, api, workloads as W
+from .batch import Batch
+from .serve import Server
+
+
+def _pct(x, q):
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def cmd_ckpt(a):
+    inst = W.large_instance(n=a.n, nt=a.nt, seed=1)
+    out = {"suite": "ckpt", "grid": a.n, "nt": a.nt}
+    for name, pol, budget in (("full", _lib.CKPT_FULL, 0), ("sqrt", _lib.CKPT_SQRT, 0),
+                              ("binomial", _lib.CKPT_BINOMIAL, a.binomial_gb * 2**30)):
+        try:
+            with api.Problem(inst, opts=api.options(ckpt_policy=pol, ckpt_budget_bytes=budget)) as pb:
+                pb.grad(inst.Et, inst.y0)
+                ms = []
+                for _ in range(a.steps):
+                    pb.grad(inst.Et)
+                    ms.append(pb.last_timing["total_ms"])
+                out[name] = {"ms_per_gradient": min(ms), "gradients_per_s": 1000.0 / min(ms),
+                             "device_bytes": pb.device_bytes, "launches": pb.last_launches}
+        except _lib.FkadjError as e:
+            out[name] = {"unavailable": str(e)}
+    print(json.dumps(out), flush=True)
+
+
+def _batch_insts(a):
+    return W.batch_instances(count=a.count, seed=a.seed, max_side=a.max_side, nt_scale=a.nt_scale)
+
+
+def cmd_batch(a):
+    insts = _batch_insts(a)
+    cells_steps = sum(i.nrows * i.ncols * i.nt for i in insts)
+    # one resident problem at a time (created, warmed, timed, freed)
+    seq = 0.0
+    for inst in insts:
+        with api.Problem(inst, opts=api.options(ckpt_policy=_lib.CKPT_SQRT)) as pb:
+            pb.grad(inst.Et, inst.y0)
+            t0 = time.perf_counter()
+            pb.grad(inst.Et)
+            seq += time.perf_counter() - t0
+    with Batch() as b:
+        pids = [b.add_problem(i, ckpt_policy=_lib.CKPT_SQRT) for i in insts]
+        jobs = [b.submit(p, i.Et, i.y0) for p, i in zip(pids, insts)]
+        b.run()
+        [b.result(j) for j in jobs]
+        t0 = time.perf_counter()
+        jobs = [b.submit(p, i.Et) for p, i in zip(pids, insts)]
+        b.run()
+        [b.result(j) for j in jobs]
+        bt = time.perf_counter() - t0
+        st = b.stats
+    print(json.dumps({"suite": "batch", "count": a.count, "max_side": a.max_side, "nt_scale": a.nt_scale,
+                      "sides": sorted({i.nrows for i in insts}), "nt_range": [min(i.nt for i in insts),
+                                                                              max(i.nt for i in insts)],
+                      "sequential_s": seq, "batched_s": bt, "speedup": seq / bt,
+                      "gradients_per_s_sequential": a.count / seq, "gradients_per_s_batched": a.count / bt,
+                      "cell_steps_per_s_batched": cells_steps / bt, "ticks": st["ticks"],
+                      "launches": st["launches"], "device_bytes": st["device_bytes"]}), flush=True)
+
+
+def cmd_serve(a):
+    rng = np.random.default_rng(a.seed)
+    base = _batch_insts(argparse.Namespace(count=a.requests, seed=a.seed, max_side=a.max_side,
+                                           nt_scale=a.nt_scale))
+    grads = [bool(x) for x in rng.integers(0, 2, size=a.requests)]
+    # standalone service time of every request (for the sequential baseline)
+    service = []
+    for inst, g in zip(base, grads):
+        with api.Problem(inst, opts=api.options(ckpt_policy=_lib.CKPT_SQRT)) as pb:
+            (pb.grad if g else pb.objective)(inst.Et, inst.y0)
+            t0 = time.perf_counter()
+            (pb.grad if g else pb.objective)(inst.Et)
+            service.append(time.perf_counter() - t0)
+    for rate in a.rates:
+        gaps = rng.exponential(1.0 / rate, size=a.requests)
+        arrive = np.cumsum(gaps) - gaps[0]
+        with Server(opts=api.options(ckpt_policy=_lib.CKPT_SQRT)) as srv:
+            t0 = time.perf_counter()
+            ids = []
+            for k, inst in enumerate(base):
+                now = time.perf_counter() - t0
+                if arrive[k] > now:
+                    time.sleep(arrive[k] - now)
+                ids.append(srv.submit(inst, want_grad=grads[k]))
+            lat = []
+            for rid in ids:
+                srv.wait(rid, 3600)
+                lat.append(srv.result(rid)["latency_s"])
+            makespan = time.perf_counter() - t0
+            peak = srv.stats["peak_running"]
+        # sequential FIFO plain solves with the same arrivals
+        fin, seq_lat = 0.0, []
+        for k in range(a.requests):
+            start = max(arrive[k], fin)
+            fin = start + service[k]
+            seq_lat.append(fin - arrive[k])
+        print(json.dumps({"suite": "serve", "rate_req_s": rate, "requests": a.requests,
+                          "max_side": a.max_side, "nt_scale": a.nt_scale,
+                          "served_p50_s": _pct(lat, 50), "served_p99_s": _pct(lat, 99),
+                          "served_throughput_req_s": a.requests / makespan,
+                          "sequential_p50_s": _pct(seq_lat, 50), "sequential_p99_s": _pct(seq_lat, 99),
+                          "sequential_throughput_req_s": a.requests / fin,
+                          "peak_running": peak}), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="fkadj.suite")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    c = sub.add_parser("ckpt")
+    c.add_argument("--n", type=int, default=512)
+    c.add_argument("--nt", type=int, default=20000)
+    c.add_argument("--steps", type=int, default=2)
+    c.add_argument("--binomial-gb", type=float, default=0.5)
+    for name in ("batch", "serve"):
+        p = sub.add_parser(name)
+        p.add_argument("--max-side", type=int, default=1024)
+        p.add_argument("--nt-scale", type=float, default=1.0)
+        p.add_argument("--seed", type=int, default=2)
+        if name == "batch":
+            p.add_argument("--count", type=int, default=64)
+        else:
+            p.add_argument("--requests", type=int, default=48)
+            p.add_argument("--rates", type=lambda s: [float(x) for x in s.split(",")], default=[10, 50, 200, 500])
+    a = ap.parse_args(argv)
+    {"ckpt": cmd_ckpt, "batch": cmd_batch, "serve": cmd_serve}[a.cmd](a)
+
+
+if __name__ == "__main__":
+    main()
