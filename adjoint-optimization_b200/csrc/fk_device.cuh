@@ -14,6 +14,14 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+// Build switches (compile-time; the defaults are the tuned choices).
+#ifndef FKADJ_HOLE_BRANCH
+#define FKADJ_HOLE_BRANCH 1
+#endif
+#ifndef FKADJ_SHARED_EXP
+#define FKADJ_SHARED_EXP 1
+#endif
+
 namespace fkadj {
 
 constexpr int HALO = 4;
@@ -26,6 +34,7 @@ struct DevModel {
     double r_tau_d, r_tau_0, r_tau_r, r_2tau_si;
     double tau_v1m, tau_v2m, r_tau_vp, r_tau_wm, r_tau_wp;
     double dv12;  // tau_v2_minus - tau_v1_minus
+    double eq;    // exp(-2 ksm (u_c - u_v)): e^{-2ksm(u-u_v)} = eq * e^{-2ksm(u-u_c)}
     double cu, cv, cw;  // D / h^2
     double dt;
 };
@@ -42,18 +51,31 @@ struct DevGrid {
 struct Step {
     double s, c;  // s and 1 - s
 };
-__device__ __forceinline__ Step smooth_step(double x) {
-    const double e = exp(-2.0 * x);
+__device__ __forceinline__ Step step_of_exp(double e) {
     const double s = 1.0 / (1.0 + e);
     return {s, isinf(e) ? 1.0 : e * s};
+}
+__device__ __forceinline__ Step smooth_step(double x) { return step_of_exp(exp(-2.0 * x)); }
+
+// p and q share the slope ksm, so q's exponential is p's times a constant:
+// one exp for both.
+__device__ __forceinline__ void steps_pq(const DevModel& P, double u, Step& sp, Step& sq) {
+#if FKADJ_SHARED_EXP
+    const double e = exp(-2.0 * (P.ksm * (u - P.u_c)));
+    sp = step_of_exp(e);
+    sq = step_of_exp(e * P.eq);
+#else
+    sp = smooth_step(P.ksm * (u - P.u_c));
+    sq = smooth_step(P.ksm * (u - P.u_v));
+#endif
 }
 
 // Ionic currents (formula of cu-F:29-45): p, q and (1 + tanh)/2 of the slow
 // inward current are the three smoothed steps.
 __device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, double w,
                                        double& ud, double& vd, double& wd) {
-    const Step sp = smooth_step(P.ksm * (u - P.u_c));
-    const Step sq = smooth_step(P.ksm * (u - P.u_v));
+    Step sp, sq;
+    steps_pq(P, u, sp, sq);
     const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
     const double p = sp.s, q = sq.s;
     const double j_fi = -v * p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
@@ -74,8 +96,8 @@ struct JacT {
 
 // 1 - tanh^2 = 4 s (1 - s) for the smoothed step s.
 __device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, double w) {
-    const Step sp = smooth_step(P.ksm * (u - P.u_c));
-    const Step sq = smooth_step(P.ksm * (u - P.u_v));
+    Step sp, sq;
+    steps_pq(P, u, sp, sq);
     const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
     const double p = sp.s, q = sq.s;
     const double dp = 4.0 * sp.s * sp.c;
@@ -104,10 +126,13 @@ template <int W, int RN>
 __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restrict__ Y, int q,
                                        double Egh, double& fu, double& fv, double& fw) {
     const double u = Y[q];
+#if FKADJ_HOLE_BRANCH
+    // holes and the NaN ring skip the arithmetic (their result is NaN either way)
     if (isnan(u)) {
         fu = fv = fw = u;
         return;
     }
+#endif
     const double v = Y[RN + q], w = Y[2 * RN + q];
     const double un = Y[q - W], us = Y[q + W], uw = Y[q - 1], ue = Y[q + 1];
     const bool nN = isnan(un), nS = !nN && isnan(us);

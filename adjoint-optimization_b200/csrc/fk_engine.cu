@@ -43,6 +43,7 @@ static DevModel make_model(const fkadj_params& p, double dt) {
     M.r_tau_wm = 1.0 / p.tau_w_minus;
     M.r_tau_wp = 1.0 / p.tau_w_plus;
     M.dv12 = p.tau_v2_minus - p.tau_v1_minus;
+    M.eq = std::exp(-2.0 * (p.ksm * (p.u_c - p.u_v)));
     M.cu = p.Du / (p.h * p.h);
     M.cv = p.Dv / (p.h * p.h);
     M.cw = p.Dw / (p.h * p.h);
@@ -1040,6 +1041,19 @@ void fkadj_problem_last_timing(const fkadj_problem* pb, double out[3]) {
 }
 
 int64_t fkadj_problem_last_launches(const fkadj_problem* pb) { return pb ? pb->impl.last_launches() : 0; }
+
+void fkadj_problem_tiles(const fkadj_problem* pb, int out[4], int shapes[12]) {
+    if (!pb || !out) return;
+    for (int k = 0; k < 4; ++k) {
+        out[k] = pb->impl.tile(k);
+        if (shapes) {
+            const fkadj::TileShape t = fkadj::tile_shape(out[k]);
+            shapes[3 * k] = t.tx;
+            shapes[3 * k + 1] = t.ty;
+            shapes[3 * k + 2] = t.nt;
+        }
+    }
+}
 
 void fkadj_problem_set_profiling(fkadj_problem* pb, int enable) {
     if (pb) pb->impl.set_profiling(enable != 0);

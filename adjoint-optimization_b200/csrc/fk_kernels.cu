@@ -24,8 +24,6 @@ namespace fkadj {
 
 namespace {
 
-constexpr double kNaN = __builtin_nan("");
-
 // Cells a thread keeps in flight per stage loop iteration (independent FP64
 // chains the scheduler can interleave).
 #ifndef FKADJ_STAGE_UNROLL
@@ -349,9 +347,12 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
         const double a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
         const int code = __ldg(wc + o);
         double ku, kv, kw;
-        if (isnan(src[s])) {
-            ku = kv = kw = kNaN;
-        } else {
+#if FKADJ_HOLE_BRANCH
+        if (isnan(src[s])) {  // holes and the NaN ring: the result is NaN
+            ku = kv = kw = src[s];
+        } else
+#endif
+        {
             JacT J;
             if (jload) {
                 J = load_jac(jload, g.plane, o);
@@ -459,9 +460,12 @@ __device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g,
         const int s = r * RW + c;
         const long long o = off + (long long)r * g.ld + c;
         double ku, kv, kw;
-        if (isnan(src[s])) {
-            ku = kv = kw = kNaN;
-        } else {
+#if FKADJ_HOLE_BRANCH
+        if (isnan(src[s])) {  // holes and the NaN ring: the result is NaN
+            ku = kv = kw = src[s];
+        } else
+#endif
+        {
             const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
             adj_at<RW, RN>(P, src, s, __ldg(wc + o), J, ku, kv, kw);
         }

@@ -176,6 +176,14 @@ class Problem:
     def set_profiling(self, on: bool = True) -> None:
         self._L.fkadj_problem_set_profiling(self._h, 1 if on else 0)
 
+    @property
+    def tiles(self):
+        """Tile shapes (tx, ty, threads) in use per kernel kind."""
+        out, shp = (C.c_int * 4)(), (C.c_int * 12)()
+        self._L.fkadj_problem_tiles(self._h, out, shp)
+        names = ("fwd_step", "adj_mid", "adj_step", "adj_exact")
+        return {n: (shp[3 * k], shp[3 * k + 1], shp[3 * k + 2]) for k, n in enumerate(names)}
+
     def kernel_time(self, kernel: int):
         """(average ms per launch, samples) of kernel 0 forward step,
         1 adjoint midpoint, 2 adjoint step, over the last call."""

@@ -217,6 +217,7 @@ def run_ours(args):
     recompute = 0 if args.ckpt == "full" else inst.nt - (inst.nt + pb_stride(inst.nt) - 1) // pb_stride(inst.nt)
     per_grad = {0: inst.nt + recompute, 1: inst.nt, 2: inst.nt}
     kt = {k: pb.kernel_time(k) for k in (0, 1, 2)}
+    tiles = pb.tiles
     share = {k: kt[k][0] * per_grad[k] for k in kt}
     dom = max(share, key=share.get)
     cells = inst.nrows * inst.ncols
@@ -229,6 +230,7 @@ def run_ours(args):
             "samples": kt[dom][1],
             "kernel_ms": {KERNEL_NAMES[k]: kt[k][0] for k in kt},
             "time_share": {KERNEL_NAMES[k]: share[k] / sum(share.values()) for k in share},
+            "tiles": {k: list(v) for k, v in tiles.items() if k != "adj_exact"},
             "note": "FP64-arithmetic bound (3 tanh per vector-field evaluation); "
                     "HBM fraction reported against the copy peak"}
     pb.close()

@@ -155,6 +155,10 @@ int64_t fkadj_problem_last_launches(const fkadj_problem *pb);
  * No reference counterpart (the reference has no timers besides tic/toc in
  * src/cuda/simple_grad_desc.m:80-86). */
 void fkadj_problem_set_profiling(fkadj_problem *pb, int enable);
+/* Tile presets in use (autotuned or fixed) for the forward step, adjoint
+ * midpoint, adjoint step and exact adjoint step: out[k] = preset index, with
+ * (tx, ty, threads) of each preset in shapes[3k..3k+2] when shapes != NULL. */
+void fkadj_problem_tiles(const fkadj_problem *pb, int out[4], int shapes[12]);
 void fkadj_problem_kernel_time(const fkadj_problem *pb, int kernel, double *avg_ms, int64_t *samples);
 
 /* ------------------------------------------------------------------------
