@@ -837,7 +837,8 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
             prev = keep;
             return FKADJ_OK;
         };
-        if ((s = reverse_binomial(0, nt, slot(0), free, visit))) return s;
+        s = reverse_binomial(0, nt, slot(0), free, visit);
+        if (s != FKADJ_OK) return s;
     } else if (tp.policy == FKADJ_CKPT_FULL) {
         for (int i = nt; i > 0; --i)
             if ((s = back_step(i, slot(i - 1), slot(i)))) return s;

@@ -59,3 +59,43 @@ def test_reference_binary_reproduces_its_golden_file(golden):
     ge = golden["gradE"][k]
     assert abs(r["Lcost"] - golden["Lcost"][k]) <= 1e-10 * golden["Lcost"][k]
     assert np.linalg.norm(r["gradE"] - ge) <= 1e-9 * np.linalg.norm(ge)
+
+
+def _timed(fn, reps):
+    import time
+    fn()                                   # warm-up (module load, first allocations)
+    t = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = fn()
+        t.append(time.perf_counter() - t0)
+    return min(t), out
+
+
+@pytest.mark.parametrize("n, nt, dx_tag", [(128, 2000, "dx0p025"), (256, 3000, "dx0p035"),
+                                           (512, 2000, "dx0p025")])
+def test_plain_solver_timing_reference_binary_vs_fkadj(n, nt, dx_tag):
+    """Wall time per gradient of the reference's own GPU code (compiled from
+    its sources; host-resident trajectory, per-step PCIe copies) beside the
+    drop-in call of this engine (same arguments, setup included) and the
+    resident problem, on the same seeded instance; gradients agree to 1e-8.
+    Prints one JSON line (run with -s to see it)."""
+    import json
+    h = 0.025 if dx_tag == "dx0p025" else 0.035
+    inst = W.make_instance(n, nt, dx=h, dt=0.02, n_obstacles=max(4, n * n // 3300), intervals=100,
+                           wavefronts=2, seed=900 + n)
+    alpha = 0.0
+    args = (inst.dt, inst.Et, inst.nt, inst.y0, inst.active_index, inst.nrows, inst.ncols, inst.ghost,
+            inst.gamma, inst.S, alpha)
+    t_ref, r = _timed(lambda: refbin.grad(*args, dx_tag=dx_tag), 2)
+    t_dropin, d = _timed(lambda: api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index,
+                                                inst.ncols, inst.nrows, inst.ghost, inst.gamma, inst.S,
+                                                alpha, params=inst.params), 3)
+    with api.Problem(inst) as pb:
+        pb.grad(inst.Et, inst.y0)
+        t_res, g = _timed(lambda: pb.grad(inst.Et, None), 3)
+    assert np.linalg.norm(d[0] - r["gradE"]) <= 1e-8 * np.linalg.norm(r["gradE"])
+    assert np.linalg.norm(g["gradE"] - r["gradE"]) <= 1e-8 * np.linalg.norm(r["gradE"])
+    print("PLAIN_SOLVER " + json.dumps({"grid": n, "nt": nt, "reference_gpu_s": t_ref, "fkadj_dropin_s": t_dropin,
+                                        "fkadj_resident_s": t_res, "speedup_dropin": t_ref / t_dropin,
+                                        "speedup_resident": t_ref / t_res}))
