@@ -120,6 +120,17 @@ __device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, d
     return J;
 }
 
+// u as the exponentials see it.  Without the hole branch, holes (NaN) reach
+// the ionic terms: they run on a finite u there, which keeps exp off its NaN
+// path, and the Laplacian / adjoint-stencil terms still make the result NaN.
+__device__ __forceinline__ double finite_u(double u) {
+#if FKADJ_HOLE_BRANCH
+    return u;
+#else
+    return isnan(u) ? 0.0 : u;
+#endif
+}
+
 // Forward vector field at shared-memory cell q of a region W doubles wide with
 // field planes RN apart: 5-point Laplacian with NaN mirroring + F_ion + E*gh.
 template <int W, int RN>
@@ -148,7 +159,7 @@ __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restri
     const double lv = P.cv * ((((a_v + b_v) + c_v) + d_v) - 4.0 * v);
     const double lw = P.cw * ((((a_w + b_w) + c_w) + d_w) - 4.0 * w);
     double ud, vd, wd;
-    fk_ion(P, u, v, w, ud, vd, wd);
+    fk_ion(P, finite_u(u), v, w, ud, vd, wd);
     fu = (lu + ud) + Egh;
     fv = lv + vd;
     fw = lw + wd;

@@ -32,8 +32,8 @@ namespace {
 constexpr int kStageUnroll = FKADJ_STAGE_UNROLL;
 
 // Resident CTAs per SM the register allocation targets: what shared memory
-// allows for the tile (101 KB at 32x32, 58 KB at 32x16 and below, one
-// 512-thread CTA).
+// allows for the tile (187 KB at 64x32: one CTA of 512 or 768 threads; 101 KB
+// at 32x32: two; 58 KB at 32x16 and below: three).
 constexpr int min_blocks(int tx, int ty, int nt) { return nt >= 512 ? 1 : (tx * ty <= 512 ? 3 : 2); }
 
 // Copies a ROWS x WIDTH window of the three planes at src (row pitch ld, plane
@@ -357,7 +357,7 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
             if (jload) {
                 J = load_jac(jload, g.plane, o);
             } else {
-                J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+                J = fk_jacT(P, finite_u(__ldg(ys + o)), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
                 if (jstore) store_jac(jstore, g.plane, o, J);
             }
             adj_at<RW, RN>(P, src, s, code, J, ku, kv, kw);
@@ -466,7 +466,8 @@ __device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g,
         } else
 #endif
         {
-            const JacT J = fk_jacT(P, __ldg(ys + o), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+            const JacT J =
+                fk_jacT(P, finite_u(__ldg(ys + o)), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
             adj_at<RW, RN>(P, src, s, __ldg(wc + o), J, ku, kv, kw);
         }
         const double la = __ldg(lamg + o), lb = __ldg(lamg + g.plane + o), lc = __ldg(lamg + 2 * g.plane + o);
@@ -760,9 +761,11 @@ static int persistent_grid(K kernel, int nt, size_t smem, int tiles) {
     X(2, 64, 32, 512)      \
     X(3, 32, 16, 256)      \
     X(4, 16, 16, 256)      \
-    X(5, 64, 16, 512)
+    X(5, 64, 16, 512)      \
+    X(6, 64, 32, 768)      \
+    X(7, 32, 32, 384)
 
-int tile_count() { return 6; }
+int tile_count() { return 8; }
 
 TileShape tile_shape(int t) {
     switch (t) {
@@ -790,6 +793,8 @@ cudaError_t kernels_init() {
         case 3: { constexpr int TX = 32, TY = 16, NT = 256; __VA_ARGS__; } break; \
         case 4: { constexpr int TX = 16, TY = 16, NT = 256; __VA_ARGS__; } break; \
         case 5: { constexpr int TX = 64, TY = 16, NT = 512; __VA_ARGS__; } break; \
+        case 6: { constexpr int TX = 64, TY = 32, NT = 768; __VA_ARGS__; } break; \
+        case 7: { constexpr int TX = 32, TY = 32, NT = 384; __VA_ARGS__; } break; \
         default: { constexpr int TX = 32, TY = 32, NT = 256; __VA_ARGS__; } break; \
     }
 

@@ -12,7 +12,9 @@ import os
 from .params import CFkParams
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libfkadj.so")
+# FKADJ_LIB selects another build of the library (a variant compiled with
+# different switches); the default is the in-tree build.
+LIB_PATH = os.environ.get("FKADJ_LIB") or os.path.join(PKG_DIR, "libfkadj.so")
 
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_NUMERIC, ERR_NODEVICE, ERR_BUSY, ERR_TIMEOUT = range(8)
 GRAD_REF, GRAD_EXACT = 0, 1
