@@ -353,7 +353,8 @@ void Problem::kernel_time(int k, double* avg_ms, int64_t* samples) const {
 
 fkadj_status Problem::step_forward(int i, const double* yin, double* yout) {
     CK(prof_begin(K_FWD), "profiling event");
-    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), Et_[i], Eh_[i], Et_[i + 1], st_),
+    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), Et_[i], Eh_[i], Et_[i + 1], st_, nullptr,
+                       ty_[T_FWD]),
        "forward step");
     CK(prof_end(K_FWD), "profiling event");
     ++launches_;
@@ -578,19 +579,28 @@ fkadj_status Problem::autotune() {
         if ((e = cudaEventSynchronize(b))) return e;
         return cudaEventElapsedTime(ms, a, b);
     };
+    // every preset at its own height; the forward step and the midpoint also
+    // with the rows that fit the grid into one wave of CTAs
     auto pick = [&](int kind, auto&& make_launch) -> cudaError_t {
         float best = 1e30f;
         for (int t = 0; t < tile_count(); ++t) {
-            float ms = 0;
-            cudaError_t e = timed([&]() { return make_launch(t); }, &ms);
-            if (e) return e;
-            launches_ += 4;
-            if (ms < best) best = ms, tk_[kind] = t;
+            int rows[2] = {0, 0}, nr = 1;  // 0 = the preset's height
+            if (kind == T_FWD || kind == T_MID) {
+                const int bal = balanced_rows(t, kind == T_FWD ? 0 : 1, g_);
+                if (bal > 0 && bal < tile_shape(t).ty) rows[nr++] = bal;
+            }
+            for (int k = 0; k < nr; ++k) {
+                float ms = 0;
+                cudaError_t e = timed([&]() { return make_launch(t, rows[k]); }, &ms);
+                if (e) return e;
+                launches_ += 4;
+                if (ms < best) best = ms, tk_[kind] = t, ty_[kind] = rows[k];
+            }
         }
         return cudaSuccess;
     };
-    cudaError_t e = pick(T_FWD, [&](int t) {
-        return launch_fwd_step(t, P_, g_, y, out, gh_.as<double>(), E, E, E, st_);
+    cudaError_t e = pick(T_FWD, [&](int t, int ty) {
+        return launch_fwd_step(t, P_, g_, y, out, gh_.as<double>(), E, E, E, st_, nullptr, ty);
     });
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_REF) {
         double* z2 = zbuf_.as<double>() + state_elems();
@@ -598,21 +608,22 @@ fkadj_status Problem::autotune() {
         double* jc = jcache_.as<double>();
         double* fc = fcache_.as<double>();
         // trial launches with the caches in use, as in the backward sweep
-        e = pick(T_MID, [&](int t) {
+        e = pick(T_MID, [&](int t, int ty) {
             return launch_adj_mid(t, P_, g_, y, y, gh_.as<double>(), yh_.as<double>(), E, E, E, hw_, st_, fc,
-                                  fc + 3 * pl, jc + 14 * pl);
+                                  fc + 3 * pl, jc + 14 * pl, ty);
         });
         if (!e)
-            e = pick(T_ADJ, [&](int t) {
+            e = pick(T_ADJ, [&](int t, int) {
                 return launch_adj_step(t, P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
                                        partial_.as<double>(), nsbx_, st_, jc, jc + 14 * pl, jc + 7 * pl);
             });
     }
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_EXACT) {
         double* z2 = zbuf_.as<double>() + state_elems();
-        e = launch_fwd_step(tk_[T_FWD], P_, g_, y, out, gh_.as<double>(), E, E, E, st_, stg_.as<double>());
+        e = launch_fwd_step(tk_[T_FWD], P_, g_, y, out, gh_.as<double>(), E, E, E, st_, stg_.as<double>(),
+                            ty_[T_FWD]);
         if (!e)
-            e = pick(T_EXACT, [&](int t) {
+            e = pick(T_EXACT, [&](int t, int) {
                 double* p = partial_.as<double>();
                 return launch_adj_exact(t, P_, g_, y, z2, y, stg_.as<double>(), wc_.as<uint8_t>(),
                                         gh_.as<double>(), p, p + nsb_, p + 2 * (size_t)nsb_, nsbx_, st_);
@@ -698,7 +709,7 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
     auto back = [&](int t, const double* y) -> fkadj_status {
         CK(prof_begin(K_FWD), "profiling event");
         CK(launch_fwd_step(tk_[T_FWD], P_, g_, y, scratch, gh_.as<double>(), Et_[t], Eh_[t], Et_[t + 1], st_,
-                           stg),
+                           stg, ty_[T_FWD]),
            "stage replay");
         CK(prof_end(K_FWD), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
@@ -806,7 +817,7 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         const int nxt = 1 - cur_c;
         CK(prof_begin(K_MID), "profiling event");
         CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), Et_[i - 1], Et_[i],
-                          E3_[i - 1], hw_, st_, have_carry ? fc[cur_c] : nullptr, fc[nxt], jh),
+                          E3_[i - 1], hw_, st_, have_carry ? fc[cur_c] : nullptr, fc[nxt], jh, ty_[T_MID]),
            "adjoint midpoint");
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
@@ -1050,7 +1061,7 @@ void fkadj_problem_tiles(const fkadj_problem* pb, int out[4], int shapes[12]) {
         if (shapes) {
             const fkadj::TileShape t = fkadj::tile_shape(out[k]);
             shapes[3 * k] = t.tx;
-            shapes[3 * k + 1] = t.ty;
+            shapes[3 * k + 1] = pb->impl.tile_rows(k);
             shapes[3 * k + 2] = t.nt;
         }
     }

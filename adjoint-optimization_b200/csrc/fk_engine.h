@@ -95,6 +95,9 @@ public:
     enum TileKind { T_FWD = 0, T_MID = 1, T_ADJ = 2, T_EXACT = 3 };
     int tile(int kind) const { return tk_[kind]; }
     void set_tile(int kind, int t) { tk_[kind] = t; }
+    // rows per tile in use for a kernel kind (the preset's height, or fewer
+    // when the autotuner found a one-wave split faster)
+    int tile_rows(int kind) const { return ty_[kind] > 0 ? ty_[kind] : tile_shape(tk_[kind]).ty; }
     // Times every tile preset of every kernel kind on the current initial
     // state (a few launches each) and keeps the fastest per kind.  Results do
     // not depend on the choice (fixed-order reductions).
@@ -136,6 +139,7 @@ private:
     double dt_ = 0, alpha_ = 0, gamma_[3] = {0, 0, 0};
     int nt_ = 0, n_num_ = 0, device_ = 0, nsbx_ = 0, nsby_ = 0, nsb_ = 0;
     int tk_[4] = {0, 0, 0, 0};  // tile preset per kernel kind (TileKind)
+    int ty_[4] = {0, 0, 0, 0};  // rows per tile per kind (0 = the preset's height)
     bool autotune_ = true, tuned_ = false, tuned_fwd_ = false;
     bool own_stream_ = false, have_obj_ = false;
     int grad_mode_ = FKADJ_GRAD_REF, ckpt_policy_ = FKADJ_CKPT_AUTO;

@@ -36,30 +36,32 @@ constexpr int kStageUnroll = FKADJ_STAGE_UNROLL;
 // at 32x32: two; 58 KB at 32x16 and below: three).
 constexpr int min_blocks(int tx, int ty, int nt) { return nt >= 512 ? 1 : (tx * ty <= 512 ? 3 : 2); }
 
-// Copies a ROWS x WIDTH window of the three planes at src (row pitch ld, plane
-// pitch plane) into shared memory (row pitch WIDTH, plane pitch ROWS*WIDTH),
-// with 16-byte vector loads when the window is 16-byte aligned.
-template <int ROWS, int WIDTH, int NT>
+// Copies a rows x WIDTH window of the three planes at src (row pitch ld, plane
+// pitch plane) into shared memory (row pitch WIDTH, plane pitch RCAP*WIDTH,
+// RCAP >= rows), with 16-byte vector loads when the window is 16-byte aligned.
+template <int RCAP, int WIDTH, int NT>
 __device__ __forceinline__ void load_region(double* __restrict__ dst, const double* __restrict__ src,
-                                            int ld, long long plane, bool vec_ok) {
-    constexpr int RN = ROWS * WIDTH;
+                                            int ld, long long plane, bool vec_ok, int rows) {
+    constexpr int RN = RCAP * WIDTH;
     if (vec_ok && (WIDTH % 2) == 0) {
         constexpr int HW = WIDTH / 2;
+        const int per = rows * HW;
 #pragma unroll 2
-        for (int q = threadIdx.x; q < 3 * ROWS * HW; q += NT) {
-            const int f = q / (ROWS * HW);
-            const int rem = q - f * (ROWS * HW);
+        for (int q = threadIdx.x; q < 3 * per; q += NT) {
+            const int f = q >= per ? (q >= 2 * per ? 2 : 1) : 0;
+            const int rem = q - f * per;
             const int r = rem / HW, c2 = rem - r * HW;
             const double2 v = __ldg(reinterpret_cast<const double2*>(src + f * plane + (long long)r * ld) + c2);
             reinterpret_cast<double2*>(dst + f * RN + r * WIDTH)[c2] = v;
         }
     } else {
+        const int per = rows * WIDTH;
 #pragma unroll 2
-        for (int q = threadIdx.x; q < 3 * RN; q += NT) {
-            const int f = q / RN;
-            const int rem = q - f * RN;
+        for (int q = threadIdx.x; q < 3 * per; q += NT) {
+            const int f = q >= per ? (q >= 2 * per ? 2 : 1) : 0;
+            const int rem = q - f * per;
             const int r = rem / WIDTH, c = rem - r * WIDTH;
-            dst[q] = __ldg(src + f * plane + (long long)r * ld + c);
+            dst[f * RN + r * WIDTH + c] = __ldg(src + f * plane + (long long)r * ld + c);
         }
     }
 }
@@ -118,10 +120,11 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
                                           double* __restrict__ dst, double* __restrict__ D,
                                           const double* __restrict__ y0g, const double* __restrict__ ghs,
                                           int ld, long long plane, double Ev, double cY, double cD,
-                                          double* __restrict__ out, double* __restrict__ stage_out) {
+                                          double* __restrict__ out, double* __restrict__ stage_out, int rows) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
-    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
+    constexpr int W = TX + 2 * E;
     constexpr int IN = TX * TY;
+    const int N = W * (rows + 2 * E);
 #pragma unroll kStageUnroll
     for (int q = threadIdx.x; q < N; q += NT) {
         const int r = HALO - E + q / W, c = HALO - E + q % W;
@@ -132,7 +135,7 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
         const double a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
         double ku, kv, kw;
         rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw);
-        const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+        const bool inner = (E == 0) || (r >= HALO && r < HALO + rows && c >= HALO && c < HALO + TX);
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
             out[o] = (a + D[d]) + cD * ku;
@@ -164,25 +167,28 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
     if (MODE != 2) __syncthreads();
 }
 
-// One RK4 step y -> y_out on tile (tbx, tby).  When `stages` is non-null the
-// stage states Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3 are stored
-// there too (three consecutive states), for the discrete-exact adjoint.
-// The tile functions may run several times per CTA (batched kernels): they
-// start by overwriting all the shared memory they read.
+// One RK4 step y -> y_out on tile (tbx, tby) of ty rows (ty <= TY; the tile
+// in the last row of tiles is cut at the grid's edge).  When `stages` is
+// non-null the stage states Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3
+// are stored there too (three consecutive states), for the discrete-exact
+// adjoint.  The tile functions may run several times per CTA (batched
+// kernels): they start by overwriting all the shared memory they read.
 template <int TX, int TY, int NT>
 __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ yin,
                                               double* __restrict__ yout, const double* __restrict__ gh, double E0,
-                                              double Eh, double E1, double* __restrict__ stages, int tbx, int tby) {
+                                              double Eh, double E1, double* __restrict__ stages, int tbx, int tby,
+                                              int ty) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
     double* B = A + 3 * RN;
     double* D = B + 3 * RN;
-    const int i0 = tby * TY, j0 = tbx * TX;
+    const int i0 = tby * ty, j0 = tbx * TX;
+    const int rows = min(ty, g.nrows - i0);
     // region origin: logical (i0 - HALO, j0 - HALO) = padded (i0, j0)
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(A, yin + off, g.ld, g.plane, vec_ok);
+    load_region<RH, RW, NT>(A, yin + off, g.ld, g.plane, vec_ok, rows + 2 * HALO);
     __syncthreads();
     const double* y0g = yin + off;
     const double* ghs = gh + off;
@@ -191,17 +197,21 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     double* s2 = stages ? stages + off : nullptr;
     double* s3 = stages ? stages + sst + off : nullptr;
     double* s4 = stages ? stages + 2 * sst + off : nullptr;
-    fwd_stage<3, TX, TY, NT, 0>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2);
-    fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3);
-    fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4);
-    fwd_stage<0, TX, TY, NT, 2>(P, B, A, D, y0g, ghs, g.ld, g.plane, E1, 0.0, dt * 1.0 / 6.0, yout + off, nullptr);
+    fwd_stage<3, TX, TY, NT, 0>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2,
+                                rows);
+    fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3,
+                                rows);
+    fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4,
+                                rows);
+    fwd_stage<0, TX, TY, NT, 2>(P, B, A, D, y0g, ghs, g.ld, g.plane, E1, 0.0, dt * 1.0 / 6.0, yout + off, nullptr,
+                                rows);
 }
 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin, double* __restrict__ yout,
-               const double* __restrict__ gh, double E0, double Eh, double E1, double* __restrict__ stages) {
-    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E0, Eh, E1, stages, blockIdx.x, blockIdx.y);
+               const double* __restrict__ gh, double E0, double Eh, double E1, double* __restrict__ stages, int ty) {
+    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E0, Eh, E1, stages, blockIdx.x, blockIdx.y, ty);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -241,23 +251,26 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
                                              const double* __restrict__ yb, const double* __restrict__ gh,
                                              double* __restrict__ yh, double Ea, double Eb, double E3,
                                              const HermiteW& hw, const double* __restrict__ fin,
-                                             double* __restrict__ fout, double* __restrict__ jh, int tbx, int tby) {
+                                             double* __restrict__ fout, double* __restrict__ jh, int tbx, int tby,
+                                             int ty) {
     constexpr int H2 = 2;
     constexpr int RW = TX + 2 * H2, RH = TY + 2 * H2, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
     double* B = A + 3 * RN;
     double* C = B + 3 * RN;
-    const int i0 = tby * TY, j0 = tbx * TX;
+    const int i0 = tby * ty, j0 = tbx * TX;
+    const int rows = min(ty, g.nrows - i0);
     // region origin: logical (i0 - 2, j0 - 2) = padded (i0 + 2, j0 + 2)
     const long long off = (long long)(i0 + HALO - H2) * g.ld + (j0 + HALO - H2);
     const bool vec_ok = ((g.ld | (j0 + HALO - H2)) & 1) == 0;
-    load_region<RH, RW, NT>(A, ya + off, g.ld, g.plane, vec_ok);
-    load_region<RH, RW, NT>(B, yb + off, g.ld, g.plane, vec_ok);
+    load_region<RH, RW, NT>(A, ya + off, g.ld, g.plane, vec_ok, rows + 2 * H2);
+    load_region<RH, RW, NT>(B, yb + off, g.ld, g.plane, vec_ok, rows + 2 * H2);
     __syncthreads();
     const double dt = P.dt;
     {
-        constexpr int W = TX + 2, N = W * (TY + 2);
+        constexpr int W = TX + 2;
+        const int N = W * (rows + 2);
 #pragma unroll kStageUnroll
         for (int q = threadIdx.x; q < N; q += NT) {
             const int r = 1 + q / W, c = 1 + q % W;
@@ -273,7 +286,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
             } else {
                 rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2]);
             }
-            const bool inner = r >= H2 && r < H2 + TY && c >= H2 && c < H2 + TX;
+            const bool inner = r >= H2 && r < H2 + rows && c >= H2 && c < H2 + TX;
             if (inner && fout) {
                 fout[o] = a0[0];
                 fout[g.plane + o] = a0[1];
@@ -292,7 +305,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
     __syncthreads();
     // C on the outer ring stays unset: stencils of tile cells reach one cell out.
     {
-        constexpr int N = TX * TY;
+        const int N = TX * rows;
 #pragma unroll kStageUnroll
         for (int q = threadIdx.x; q < N; q += NT) {
             const int r = H2 + q / TX, c = H2 + q % TX;
@@ -315,8 +328,8 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya, const double* __restrict__ yb,
               const double* __restrict__ gh, double* __restrict__ yh, double Ea, double Eb, double E3, HermiteW hw,
-              const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh) {
-    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, blockIdx.x, blockIdx.y);
+              const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty) {
+    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, blockIdx.x, blockIdx.y, ty);
 }
 
 // One adjoint stage on the tile grown by E cells: k = L^T src + J_F(y)^T src,
@@ -413,7 +426,7 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(A, z + off, g.ld, g.plane, vec_ok);
+    load_region<RH, RW, NT>(A, z + off, g.ld, g.plane, vec_ok, RH);
     __syncthreads();
     const double dt = P.dt;
     adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb, nullptr);
@@ -519,7 +532,7 @@ __device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid&
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(A, lam + off, g.ld, g.plane, vec_ok);
+    load_region<RH, RW, NT>(A, lam + off, g.ld, g.plane, vec_ok, RH);
     __syncthreads();
     const double dt = P.dt;
     const double c6 = dt / 6.0, c3 = dt / 3.0, c2 = dt * 0.5;
@@ -582,7 +595,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
-        fwd_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, I.gh, it.E0, it.E1, it.E2, it.stages, tbx, tby);
+        fwd_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, I.gh, it.E0, it.E1, it.E2, it.stages, tbx, tby, TY);
     }
 }
 
@@ -595,7 +608,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
         adj_mid_tile<TX, TY, NT>(I.P, I.g, it.a, it.b, I.gh, it.out, it.E0, it.E1, it.E2, hw, it.fin, it.fout,
-                                 it.jh, tbx, tby);
+                                 it.jh, tbx, tby, TY);
     }
 }
 
@@ -804,9 +817,12 @@ static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
 
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, double E0, double Eh, double E1, cudaStream_t st,
-                            double* stages) {
-    DISPATCH(tile, (k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT), st>>>(
-                        P, g, yin, yout, gh, E0, Eh, E1, stages)));
+                            double* stages, int ty) {
+    DISPATCH(tile, {
+        const int rows = (ty > 0 && ty < TY) ? ty : TY;
+        k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, rows), NT, stencil_smem<TX, TY>(NT), st>>>(
+            P, g, yin, yout, gh, E0, Eh, E1, stages, rows);
+    });
     return cudaGetLastError();
 }
 
@@ -820,10 +836,40 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
 
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
-                           cudaStream_t st, const double* fin, double* fout, double* jh) {
-    DISPATCH(tile, (k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, TY), NT, mid_smem<TX, TY>(), st>>>(
-                        P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh)));
+                           cudaStream_t st, const double* fin, double* fout, double* jh, int ty) {
+    DISPATCH(tile, {
+        const int rows = (ty > 0 && ty < TY) ? ty : TY;
+        k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, rows), NT, mid_smem<TX, TY>(), st>>>(
+            P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, rows);
+    });
     return cudaGetLastError();
+}
+
+// Rows per tile that spread the grid over one wave of CTAs (occupancy x SMs)
+// with as little work per CTA as the preset's width allows; the preset's own
+// height when the grid needs more than one wave at that height.
+template <class K>
+static int wave_rows(K kernel, int nt, size_t smem, int tx, int ty, const DevGrid& g) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        return ty;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, smem) != cudaSuccess || per_sm < 1)
+        return ty;
+    const int ntx = (g.ncols + tx - 1) / tx;
+    const int nty = (sms * per_sm) / ntx;
+    if (nty < 1) return ty;
+    const int rows = (g.nrows + nty - 1) / nty;
+    return rows < ty ? rows : ty;
+}
+
+int balanced_rows(int tile, int kind, const DevGrid& g) {
+    int r = 0;
+    DISPATCH(tile, {
+        r = kind == 0 ? wave_rows(k_fwd_step<TX, TY, NT>, NT, stencil_smem<TX, TY>(NT), TX, TY, g)
+                      : wave_rows(k_adj_mid<TX, TY, NT>, NT, mid_smem<TX, TY>(), TX, TY, g);
+    });
+    return r;
 }
 
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,

@@ -69,9 +69,15 @@ TileShape tile_shape(int tile);
 int tiles_of(int tile, const DevGrid& g);
 cudaError_t kernels_init();
 
+// ty: rows per tile, 0 < ty < the preset's height, or 0 for the preset's
+// height (forward step and adjoint midpoint only).
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, double E0, double Eh, double E1, cudaStream_t st,
-                            double* stages = nullptr);
+                            double* stages = nullptr, int ty = 0);
+// Rows per tile that fit grid g into one wave of CTAs of preset `tile` for
+// kernel kind 0 (forward step) or 1 (adjoint midpoint); the preset's height
+// when it does not fit.
+int balanced_rows(int tile, int kind, const DevGrid& g);
 // The z.gh style reductions write one partial per 16x16 sub-block of the
 // grid's lattice (nsbx x nsby, covering the 64-padded grid); sub-blocks no
 // tile covers are never written and must be zero.
@@ -82,7 +88,7 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
                            cudaStream_t st, const double* fin = nullptr, double* fout = nullptr,
-                           double* jh = nullptr);
+                           double* jh = nullptr, int ty = 0);
 // jb: cached J(y_i) (null = evaluate), jh: cached J(yh) (null = evaluate),
 // ja: where J(y_{i-1}) is stored for the next step (null = not kept).
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
