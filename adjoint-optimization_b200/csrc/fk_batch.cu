@@ -202,6 +202,7 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
                       "standalone engine (raise ckpt_budget_bytes or use fkadj_problem_grad)");
             return FKADJ_ERR_NOMEM;
         }
+        j->tp.keep_f = false;  // the batched midpoint evaluates f itself
         if ((s = P.ensure_traj(j->tp))) return s;
         if ((s = P.ensure_adjoint_work())) return s;
         if ((s = P.upload_state(y_ini, P.slot(0)))) return s;
@@ -264,8 +265,14 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
     const size_t nsb = (size_t)P.nsb_;
     const int c = j.tp.stride, K = j.tp.nslots - 1;
     const bool full = j.tp.policy == FKADJ_CKPT_FULL;
-    const TileShape ts = tile_shape(tiles_[0]);
-    const int ntx = (P.g_.ncols + ts.tx - 1) / ts.tx, nty = (P.g_.nrows + ts.ty - 1) / ts.ty;
+    // each kernel kind runs its own tile preset: the queue of kind k is cut
+    // into tiles of that preset
+    auto ntiles = [&](const BatchTick* T, int& ntx) {
+        const int k = T == t_fwd_ ? 0 : (T == t_mid_ ? 1 : 2);
+        const TileShape ts = tile_shape(tiles_[k]);
+        ntx = (P.g_.ncols + ts.tx - 1) / ts.tx;
+        return ntx * ((P.g_.nrows + ts.ty - 1) / ts.ty);
+    };
     auto seg = [&](int t, int k) -> double* {  // backward-sweep state store
         if (full) return P.slot(t);
         const int s0 = k * c, s1 = std::min(s0 + c, nt);
@@ -274,11 +281,13 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
         return P.segslot(t - s0 - 1);
     };
     auto push = [&](BatchTick* T, BatchItem it) {
+        int ntx = 1;
+        const int n = ntiles(T, ntx);
         it.inst = j.prob;
         it.tile0 = T->tiles;
         it.ntx = ntx;
         T->item[T->n++] = it;
-        T->tiles += ntx * nty;
+        T->tiles += n;
     };
     BatchItem it{};
     switch (a.kind) {

@@ -264,7 +264,7 @@ int64_t Problem::estimate_bytes(int nrows, int ncols, int nt, int n_num, int64_t
 
 int64_t Problem::device_bytes() const {
     const DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_,
-                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &y0res_, &stg_, &jcache_, &fcache_};
+                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_, &fcache_};
     int64_t s = 0;
     for (auto* b : all) s += (int64_t)b->bytes;
     return s;
@@ -351,10 +351,10 @@ void Problem::kernel_time(int k, double* avg_ms, int64_t* samples) const {
     if (samples) *samples = ksamples_[k];
 }
 
-fkadj_status Problem::step_forward(int i, const double* yin, double* yout) {
+fkadj_status Problem::step_forward(int i, const double* yin, double* yout, double* k1) {
     CK(prof_begin(K_FWD), "profiling event");
     CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), Et_[i], Eh_[i], Et_[i + 1], st_, nullptr,
-                       ty_[T_FWD]),
+                       ty_[T_FWD], k1),
        "forward step");
     CK(prof_end(K_FWD), "profiling event");
     ++launches_;
@@ -515,20 +515,34 @@ fkadj_status Problem::plan_trajectory(TrajPlan& tp) {
         set_error("trajectory store does not fit the checkpoint budget");
         return FKADJ_ERR_NOMEM;
     }
+    // reference mode: keep k1 = f(y) beside the states the backward sweep walks
+    // (the midpoint kernel then reads it instead of evaluating it) when that
+    // also fits the budget
+    if (grad_mode_ == FKADJ_GRAD_REF && pol != FKADJ_CKPT_BINOMIAL) {
+        const double kslots = pol == FKADJ_CKPT_FULL ? (double)nt_ : (double)tp.seg_slots;
+        tp.keep_f = need + kslots * sb <= (double)ckpt_budget_;
+    }
     return FKADJ_OK;
 }
 
 fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
     if (traj_.p && traj_plan_.policy == tp.policy && traj_plan_.nslots == tp.nslots &&
-        traj_plan_.seg_slots == tp.seg_slots)
+        traj_plan_.seg_slots == tp.seg_slots && traj_plan_.keep_f == tp.keep_f)
         return FKADJ_OK;
     traj_.release();
     seg_.release();
+    kf_.release();
     CK(traj_.alloc((size_t)tp.nslots * state_bytes()), "alloc trajectory");
     CK(cudaMemsetAsync(traj_.p, 0xff, traj_.bytes, st_), "init trajectory");
     if (tp.seg_slots) {
         CK(seg_.alloc((size_t)tp.seg_slots * state_bytes()), "alloc segment buffer");
         CK(cudaMemsetAsync(seg_.p, 0xff, seg_.bytes, st_), "init segment buffer");
+    }
+    if (tp.keep_f) {
+        // cells no tile writes (ring, padding) stay NaN, as f there is
+        const size_t k = tp.policy == FKADJ_CKPT_FULL ? (size_t)nt_ : (size_t)tp.seg_slots;
+        CK(kf_.alloc(k * state_bytes()), "alloc kept f");
+        CK(cudaMemsetAsync(kf_.p, 0xff, kf_.bytes, st_), "init kept f");
     }
     traj_plan_ = tp;
     return FKADJ_OK;
@@ -782,7 +796,8 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         else if ((i + 1) % c == 0) out = slot((i + 1) / c);
         else if (i + 1 == nt) out = slot(K);
         else out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
-        if ((s = step_forward(i, cur, out))) return s;
+        double* k1 = (tp.policy == FKADJ_CKPT_FULL && tp.keep_f) ? fslot(i) : nullptr;
+        if ((s = step_forward(i, cur, out, k1))) return s;
         cur = out;
     }
     double* yT = cur;
@@ -811,25 +826,30 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     double* jy[2] = {jcache_.as<double>(), jcache_.as<double>() + 7 * pl};
     double* jh = jcache_.as<double>() + 14 * pl;
     double* fc[2] = {fcache_.as<double>(), fcache_.as<double>() + 3 * pl};
-    bool have_carry = false;
+    // fa / fb: kept k1 = f(y_{i-1}) / f(y_i) (null = not kept).  The f carry
+    // is valid only after a step that evaluated f(y_{i-1}) itself.
+    bool have_fcarry = false, have_jcarry = false;
     int cur_c = 0;
-    auto back_step = [&](int i, const double* ya, const double* yb) -> fkadj_status {
+    auto back_step = [&](int i, const double* ya, const double* yb, const double* fa,
+                         const double* fb) -> fkadj_status {
         const int nxt = 1 - cur_c;
+        const double* fin = fb ? fb : (have_fcarry ? fc[cur_c] : nullptr);
         CK(prof_begin(K_MID), "profiling event");
         CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), Et_[i - 1], Et_[i],
-                          E3_[i - 1], hw_, st_, have_carry ? fc[cur_c] : nullptr, fc[nxt], jh, ty_[T_MID]),
+                          E3_[i - 1], hw_, st_, fin, fa ? nullptr : fc[nxt], jh, ty_[T_MID], fa),
            "adjoint midpoint");
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
                            gh_.as<double>(), part + (size_t)(i - 1) * nsb, nsbx_, st_,
-                           have_carry ? jy[cur_c] : nullptr, jh, jy[nxt]),
+                           have_jcarry ? jy[cur_c] : nullptr, jh, jy[nxt]),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
         std::swap(z, z2);
         cur_c = nxt;
-        have_carry = true;
+        have_fcarry = fa == nullptr;
+        have_jcarry = true;
         return FKADJ_OK;
     };
     if (exact) {
@@ -842,7 +862,7 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         const double* prev = slot(1);  // y(T)
         double* keep = state_buf(0);
         auto visit = [&](int j, const double* yj) -> fkadj_status {
-            fkadj_status r = back_step(j + 1, yj, prev);
+            fkadj_status r = back_step(j + 1, yj, prev, nullptr, nullptr);
             if (r) return r;
             CK(cudaMemcpyAsync(keep, yj, state_bytes(), cudaMemcpyDeviceToDevice, st_), "keep state");
             prev = keep;
@@ -851,8 +871,12 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         s = reverse_binomial(0, nt, slot(0), free, visit);
         if (s != FKADJ_OK) return s;
     } else if (tp.policy == FKADJ_CKPT_FULL) {
-        for (int i = nt; i > 0; --i)
-            if ((s = back_step(i, slot(i - 1), slot(i)))) return s;
+        // kept: f(y_t) for t < nt
+        for (int i = nt; i > 0; --i) {
+            const double* fa = tp.keep_f ? fslot(i - 1) : nullptr;
+            const double* fb = (tp.keep_f && i < nt) ? fslot(i) : nullptr;
+            if ((s = back_step(i, slot(i - 1), slot(i), fa, fb))) return s;
+        }
     } else {
         for (int k = K - 1; k >= 0; --k) {
             const int s0 = k * c, s1 = std::min(s0 + c, nt);
@@ -861,10 +885,14 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
                 if (t == s1) return slot(k + 1);
                 return segslot(t - s0 - 1);
             };
+            // the recompute keeps f(y_t) for t = s0 .. s1-2 in fslot(t - s0)
+            auto kept = [&](int t) -> double* {
+                return (tp.keep_f && t >= s0 && t <= s1 - 2) ? fslot(t - s0) : nullptr;
+            };
             for (int t = s0; t < s1 - 1; ++t)
-                if ((s = step_forward(t, st(t), st(t + 1)))) return s;
+                if ((s = step_forward(t, st(t), st(t + 1), kept(t)))) return s;
             for (int i = s1; i > s0; --i)
-                if ((s = back_step(i, st(i - 1), st(i)))) return s;
+                if ((s = back_step(i, st(i - 1), st(i), kept(i - 1), kept(i)))) return s;
         }
     }
     const int rows = exact ? 3 * nt : nt + 1;

@@ -53,6 +53,8 @@ struct TrajPlan {
     int stride = 1;                // steps between stored states (SQRT)
     int nslots = 0;                // stored state slots
     int seg_slots = 0;             // recompute buffer slots
+    bool keep_f = false;           // k1 = f(y_t, Et[t]) kept beside the states the
+                                   // backward sweep walks (FULL: all, SQRT: the segment)
 };
 
 class BatchEngine;
@@ -108,7 +110,7 @@ public:
     // previous call (kept resident on the device).
     fkadj_status upload_state(const double* y_ini, double* d_state);
     fkadj_status prepare_E(const double* Et);
-    fkadj_status step_forward(int i, const double* yin, double* yout);
+    fkadj_status step_forward(int i, const double* yin, double* yout, double* k1 = nullptr);
     double* state_buf(int k) const { return work_.as<double>() + (size_t)k * state_elems(); }
     size_t state_elems() const { return (size_t)3 * g_.plane; }
     size_t state_bytes() const { return state_elems() * sizeof(double); }
@@ -131,6 +133,7 @@ private:
     fkadj_status download_grid(const double* d_state, double* host_dense);
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
     double* segslot(int k) const { return seg_.as<double>() + (size_t)k * state_elems(); }
+    double* fslot(int k) const { return kf_.as<double>() + (size_t)k * state_elems(); }
 
     fkadj_params p_{};
     DevModel P_{};
@@ -155,6 +158,7 @@ private:
     DevBuf partial_;   // (nt+1) x ntiles zgh partials
     DevBuf zgh_;       // nt+1
     DevBuf traj_, seg_;
+    DevBuf kf_;        // kept k1 = f(y_t) per stored / recomputed state (TrajPlan::keep_f)
     DevBuf y0res_;     // resident initial state
     DevBuf stg_;       // stage states Y2, Y3, Y4 of one step (exact mode)
     DevBuf jcache_;    // cached Jacobians (reference mode): J(y) ping-pong + J(yh)

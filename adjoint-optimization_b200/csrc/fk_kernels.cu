@@ -120,7 +120,8 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
                                           double* __restrict__ dst, double* __restrict__ D,
                                           const double* __restrict__ y0g, const double* __restrict__ ghs,
                                           int ld, long long plane, double Ev, double cY, double cD,
-                                          double* __restrict__ out, double* __restrict__ stage_out, int rows) {
+                                          double* __restrict__ out, double* __restrict__ stage_out, int rows,
+                                          double* __restrict__ k_out = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E;
     constexpr int IN = TX * TY;
@@ -161,6 +162,11 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
                     stage_out[plane + o] = nv;
                     stage_out[2 * plane + o] = nw;
                 }
+                if (MODE == 0 && k_out) {  // k1 = f(y, E0), kept for the adjoint midpoint
+                    k_out[o] = ku;
+                    k_out[plane + o] = kv;
+                    k_out[2 * plane + o] = kw;
+                }
             }
         }
     }
@@ -171,13 +177,13 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
 // in the last row of tiles is cut at the grid's edge).  When `stages` is
 // non-null the stage states Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3
 // are stored there too (three consecutive states), for the discrete-exact
-// adjoint.  The tile functions may run several times per CTA (batched
+// adjoint; when `k1` is non-null, k1 = f(y, E0) is stored there (a state).  The tile functions may run several times per CTA (batched
 // kernels): they start by overwriting all the shared memory they read.
 template <int TX, int TY, int NT>
 __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ yin,
                                               double* __restrict__ yout, const double* __restrict__ gh, double E0,
                                               double Eh, double E1, double* __restrict__ stages, int tbx, int tby,
-                                              int ty) {
+                                              int ty, double* __restrict__ k1 = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -198,7 +204,7 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     double* s3 = stages ? stages + sst + off : nullptr;
     double* s4 = stages ? stages + 2 * sst + off : nullptr;
     fwd_stage<3, TX, TY, NT, 0>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2,
-                                rows);
+                                rows, k1 ? k1 + off : nullptr);
     fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3,
                                 rows);
     fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4,
@@ -210,8 +216,9 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin, double* __restrict__ yout,
-               const double* __restrict__ gh, double E0, double Eh, double E1, double* __restrict__ stages, int ty) {
-    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E0, Eh, E1, stages, blockIdx.x, blockIdx.y, ty);
+               const double* __restrict__ gh, double E0, double Eh, double E1, double* __restrict__ stages, int ty,
+               double* __restrict__ k1) {
+    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E0, Eh, E1, stages, blockIdx.x, blockIdx.y, ty, k1);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -245,6 +252,8 @@ __device__ __forceinline__ void store_jac(double* __restrict__ Jb, long long pla
 // Work shared between consecutive backward steps (same values, computed once):
 //   f(yb, Eb) of step i is f(ya, Ea) of step i+1: when fin is non-null it is
 //   read from there instead of evaluated, and f(ya, Ea) goes to fout;
+//   f(ya, Ea) is k1 of the forward step from ya: when fa is non-null (the
+//   forward recompute kept it) it is read from there too;
 //   J_F(yh)^T, used by stages 2 and 3 of the adjoint step, goes to jh.
 template <int TX, int TY, int NT>
 __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ ya,
@@ -252,7 +261,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
                                              double* __restrict__ yh, double Ea, double Eb, double E3,
                                              const HermiteW& hw, const double* __restrict__ fin,
                                              double* __restrict__ fout, double* __restrict__ jh, int tbx, int tby,
-                                             int ty) {
+                                             int ty, const double* __restrict__ fa = nullptr) {
     constexpr int H2 = 2;
     constexpr int RW = TX + 2 * H2, RH = TY + 2 * H2, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
@@ -278,7 +287,13 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
             const long long o = off + (long long)r * g.ld + c;
             const double gg = __ldg(gh + o);
             double a0[3], a1[3];
-            rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2]);
+            if (fa) {
+                a0[0] = __ldg(fa + o);
+                a0[1] = __ldg(fa + g.plane + o);
+                a0[2] = __ldg(fa + 2 * g.plane + o);
+            } else {
+                rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2]);
+            }
             if (fin) {
                 a1[0] = __ldg(fin + o);
                 a1[1] = __ldg(fin + g.plane + o);
@@ -328,8 +343,9 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya, const double* __restrict__ yb,
               const double* __restrict__ gh, double* __restrict__ yh, double Ea, double Eb, double E3, HermiteW hw,
-              const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty) {
-    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, blockIdx.x, blockIdx.y, ty);
+              const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty,
+              const double* __restrict__ fa) {
+    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, blockIdx.x, blockIdx.y, ty, fa);
 }
 
 // One adjoint stage on the tile grown by E cells: k = L^T src + J_F(y)^T src,
@@ -817,11 +833,11 @@ static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
 
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, double E0, double Eh, double E1, cudaStream_t st,
-                            double* stages, int ty) {
+                            double* stages, int ty, double* k1) {
     DISPATCH(tile, {
         const int rows = (ty > 0 && ty < TY) ? ty : TY;
         k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, rows), NT, stencil_smem<TX, TY>(NT), st>>>(
-            P, g, yin, yout, gh, E0, Eh, E1, stages, rows);
+            P, g, yin, yout, gh, E0, Eh, E1, stages, rows, k1);
     });
     return cudaGetLastError();
 }
@@ -836,11 +852,12 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
 
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
-                           cudaStream_t st, const double* fin, double* fout, double* jh, int ty) {
+                           cudaStream_t st, const double* fin, double* fout, double* jh, int ty,
+                           const double* fa) {
     DISPATCH(tile, {
         const int rows = (ty > 0 && ty < TY) ? ty : TY;
         k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, rows), NT, mid_smem<TX, TY>(), st>>>(
-            P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, rows);
+            P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, rows, fa);
     });
     return cudaGetLastError();
 }

@@ -70,10 +70,12 @@ int tiles_of(int tile, const DevGrid& g);
 cudaError_t kernels_init();
 
 // ty: rows per tile, 0 < ty < the preset's height, or 0 for the preset's
-// height (forward step and adjoint midpoint only).
+// height (forward step and adjoint midpoint only).  k1 (forward step): where
+// k1 = f(y, E0) is kept (a state, null = not kept).  fa (midpoint): f(ya, Ea)
+// as kept by the forward step from ya (null = evaluate).
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, double E0, double Eh, double E1, cudaStream_t st,
-                            double* stages = nullptr, int ty = 0);
+                            double* stages = nullptr, int ty = 0, double* k1 = nullptr);
 // Rows per tile that fit grid g into one wave of CTAs of preset `tile` for
 // kernel kind 0 (forward step) or 1 (adjoint midpoint); the preset's height
 // when it does not fit.
@@ -88,7 +90,7 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
                            cudaStream_t st, const double* fin = nullptr, double* fout = nullptr,
-                           double* jh = nullptr, int ty = 0);
+                           double* jh = nullptr, int ty = 0, const double* fa = nullptr);
 // jb: cached J(y_i) (null = evaluate), jh: cached J(yh) (null = evaluate),
 // ja: where J(y_{i-1}) is stored for the next step (null = not kept).
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
