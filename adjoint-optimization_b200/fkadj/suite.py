@@ -52,6 +52,8 @@ def cmd_ckpt(a):
 
 
 def _batch_insts(a):
+    if a.side > 0:  # `count` instances of one size, each with its own seeded geometry and pulse
+        return [W.make_instance(a.side, a.nt, seed=100 + k, n_obstacles=8, intervals=20) for k in range(a.count)]
     return W.batch_instances(count=a.count, seed=a.seed, max_side=a.max_side, nt_scale=a.nt_scale)
 
 
@@ -78,6 +80,7 @@ def cmd_batch(a):
         bt = time.perf_counter() - t0
         st = b.stats
     print(json.dumps({"suite": "batch", "count": a.count, "max_side": a.max_side, "nt_scale": a.nt_scale,
+                      "uniform": a.side > 0,
                       "sides": sorted({i.nrows for i in insts}), "nt_range": [min(i.nt for i in insts),
                                                                               max(i.nt for i in insts)],
                       "sequential_s": seq, "batched_s": bt, "speedup": seq / bt,
@@ -146,6 +149,8 @@ def main(argv=None):
         p.add_argument("--seed", type=int, default=2)
         if name == "batch":
             p.add_argument("--count", type=int, default=64)
+            p.add_argument("--side", type=int, default=0, help="uniform batch: grid side (0 = uneven mix)")
+            p.add_argument("--nt", type=int, default=2000, help="uniform batch: steps")
         else:
             p.add_argument("--requests", type=int, default=48)
             p.add_argument("--rates", type=lambda s: [float(x) for x in s.split(",")], default=[10, 50, 200, 500])

@@ -43,10 +43,15 @@ for _p in (PKG, os.path.join(ROOT, "oracle")):
 METRIC = "fwd+adjoint gradients/s at 512^2"
 UNIT = "gradients/s"
 
-# algorithmic bytes per dense cell per launch (one RK4 step of the unit)
+# bytes per dense cell per launch the kernels move as designed (one RK4 step)
 BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
-                  1: 80.0,    # adjoint midpoint: read y_i, y_{i-1} (48) + gh (8), write yh (24)
-                  2: 128.0}   # adjoint step: read z, y_i, yh, y_{i-1} (96) + gh (8), write z (24)
+                  1: 184.0,   # adjoint midpoint: read y_{i-1}, y_i (48) + f(y_{i-1}), f(y_i) (48) + gh (8),
+                              #   write yh (24) + J(yh) (56)
+                  2: 249.0}   # adjoint step: read z (24) + J(y_i), J(yh) (112) + y_{i-1} (24) + gh (8)
+                              #   + weight code (1), write z (24) + J(y_{i-1}) (56)
+# DRAM bytes per cell of one k_fwd_step launch measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, cold L2) at 512x512: profiles/k_fwd_step_512x512_traffic.md
+FWD_TRAFFIC_PER_CELL = None
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
 
 
@@ -231,9 +236,34 @@ def run_ours(args):
             "kernel_ms": {KERNEL_NAMES[k]: kt[k][0] for k in kt},
             "time_share": {KERNEL_NAMES[k]: share[k] / sum(share.values()) for k in share},
             "tiles": {k: list(v) for k, v in tiles.items() if k != "adj_exact"},
-            "note": "FP64-arithmetic bound (3 tanh per vector-field evaluation); "
-                    "HBM fraction reported against the copy peak"}
+            "note": "FP64 bound: a vector-field evaluation costs 2 exp, 3 reciprocals, 1 divide and ~60 "
+                    "FMA-class operations, 4.6 evaluations per cell-step; the HBM fraction is reported "
+                    "against the copy peak"}
+    if roof["traffic"] is None and dom == 0 and FWD_TRAFFIC_PER_CELL:
+        roof["traffic"] = FWD_TRAFFIC_PER_CELL * cells
+        roof["traffic_source"] = "ncu capture, profiles/k_fwd_step_512x512_traffic.md"
+    sqrt_bytes = pb.device_bytes
     pb.close()
+
+    # the other trajectory store of the configuration: the full trajectory on the device
+    full = None
+    if not args.no_full and args.ckpt != "full" and world == 1:
+        try:
+            fopts = api.options(ckpt_policy=_lib.CKPT_FULL, stream=stream.cuda_stream, device=local, tile=args.tile)
+            with api.Problem(inst, opts=fopts) as pf:
+                pf.grad(Et, inst.y0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for _ in range(args.full_steps):
+                    pf.grad(Et)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                fms = e0.elapsed_time(e1) / args.full_steps
+                full = {"value": 1000.0 / fms, "unit": UNIT, "ms_per_step": fms, "steps": args.full_steps,
+                        "device_bytes": pf.device_bytes, "sqrt_device_bytes": sqrt_bytes}
+        except _lib.FkadjError as e:
+            full = {"unavailable": str(e)}
 
     # e2e through the drop-in C ABI (fkadj_grad), host buffers in pinned memory
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -266,6 +296,8 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": workload_config(args, inst, args.ckpt), "roofline": roof, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        if full is not None:
+            line["full_storage"] = full
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -291,6 +323,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-full", action="store_true", help="skip the full-trajectory comparison")
+    ap.add_argument("--full-steps", type=int, default=2)
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if captured")
     args = ap.parse_args()
