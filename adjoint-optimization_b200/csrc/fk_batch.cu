@@ -193,7 +193,7 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
     j->want_grad = want_grad;
     j->t_submit = host_seconds();
     fkadj_status s;
-    if ((s = P.prepare_E(Et))) return s;
+    if ((s = P.prepare_E(Et, false))) return s;  // batched kernels take E by value
     j->Et.assign(Et, Et + P.nt_ + 1);
     if (want_grad) {
         if ((s = P.plan_trajectory(j->tp))) return s;

@@ -82,8 +82,26 @@ Problem::~Problem() {
     }
     for (auto& e : ev_)
         if (e) cudaEventDestroy(e);
+    drop_graph();
+    if (Ehost_) cudaFreeHost(Ehost_);
+    if (hres_) cudaFreeHost(hres_);
     if (own_stream_ && st_) cudaStreamDestroy(st_);
     delete spline_;
+}
+
+bool Problem::GraphKey::operator==(const GraphKey& o) const {
+    if (policy != o.policy || nslots != o.nslots || seg_slots != o.seg_slots || keep_f != o.keep_f ||
+        exact != o.exact || gen != o.gen)
+        return false;
+    for (int k = 0; k < 4; ++k)
+        if (tk[k] != o.tk[k] || ty[k] != o.ty[k]) return false;
+    return true;
+}
+
+void Problem::drop_graph() {
+    if (gexec_) cudaGraphExecDestroy(gexec_);
+    gexec_ = nullptr;
+    gkey_ = GraphKey{};
 }
 
 fkadj_status Problem::fail_cuda(cudaError_t e, const char* what) {
@@ -154,6 +172,12 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
         own_stream_ = true;
     }
     for (auto& e : ev_) CK(cudaEventCreate(&e), "cudaEventCreate");
+    {
+        // stream capture needs a real stream; FKADJ_NO_GRAPHS=1 keeps plain launches
+        const char* ng = getenv("FKADJ_NO_GRAPHS");
+        graphs_ = st_ != nullptr && st_ != cudaStreamLegacy && st_ != cudaStreamPerThread &&
+                  !(ng && ng[0] && ng[0] != '0');
+    }
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
     ckpt_budget_ = o.ckpt_budget_bytes > 0 ? o.ckpt_budget_bytes : (int64_t)(0.6 * (double)fr);
@@ -270,7 +294,7 @@ int64_t Problem::device_bytes() const {
     return s;
 }
 
-fkadj_status Problem::prepare_E(const double* Et) {
+fkadj_status Problem::prepare_E(const double* Et, bool upload) {
     for (int k = 0; k < K_COUNT; ++k) kcount_[k] = ksamples_[k] = 0, kms_[k] = 0.0;
     prof_used_ = 0;
     prof_every_ = std::max(1, nt_ / 100);
@@ -287,6 +311,20 @@ fkadj_status Problem::prepare_E(const double* Et) {
         Eh_[i] = spline_->value(Et_.data(), ypp_.data(), (i + 0.5) * dt_);          // cu-G:1692-1694
         E3_[i] = spline_->value(Et_.data(), ypp_.data(), (i + 1.0 / 3.0) * dt_);    // cu-G:1877-1879
     }
+    if (!upload) return FKADJ_OK;
+    // device tables [Et | Eh | E3] for the kernels (through pinned staging)
+    const size_t n = (size_t)3 * nt_ + 1;
+    if (!Ed_.p) {
+        CK(Ed_.alloc(n * sizeof(double)), "alloc E tables");
+        CK(cudaMallocHost(&Ehost_, n * sizeof(double)), "alloc pinned E tables");
+        ++buf_gen_;
+    } else {
+        CK(cudaStreamSynchronize(st_), "synchronize");  // the previous upload is done with the staging
+    }
+    std::copy(Et_.begin(), Et_.end(), Ehost_);
+    std::copy(Eh_.begin(), Eh_.end(), Ehost_ + nt_ + 1);
+    std::copy(E3_.begin(), E3_.end(), Ehost_ + 2 * nt_ + 1);
+    CK(cudaMemcpyAsync(Ed_.p, Ehost_, n * sizeof(double), cudaMemcpyHostToDevice, st_), "upload E tables");
     return FKADJ_OK;
 }
 
@@ -353,8 +391,7 @@ void Problem::kernel_time(int k, double* avg_ms, int64_t* samples) const {
 
 fkadj_status Problem::step_forward(int i, const double* yin, double* yout, double* k1) {
     CK(prof_begin(K_FWD), "profiling event");
-    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), Et_[i], Eh_[i], Et_[i + 1], st_, nullptr,
-                       ty_[T_FWD], k1),
+    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), efwd(i), st_, nullptr, ty_[T_FWD], k1),
        "forward step");
     CK(prof_end(K_FWD), "profiling event");
     ++launches_;
@@ -529,6 +566,8 @@ fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
     if (traj_.p && traj_plan_.policy == tp.policy && traj_plan_.nslots == tp.nslots &&
         traj_plan_.seg_slots == tp.seg_slots && traj_plan_.keep_f == tp.keep_f)
         return FKADJ_OK;
+    drop_graph();
+    ++buf_gen_;
     traj_.release();
     seg_.release();
     kf_.release();
@@ -572,6 +611,13 @@ fkadj_status Problem::ensure_adjoint_work() {
         CK(partial_.alloc(pbytes), "alloc partials");
         CK(cudaMemsetAsync(partial_.p, 0, partial_.bytes, st_), "zero partials");
         CK(zgh_.alloc(prow * sizeof(double)), "alloc zgh");
+        ++buf_gen_;
+    }
+    if (hres_n_ < prow + 1) {
+        if (hres_) cudaFreeHost(hres_);
+        hres_ = nullptr;
+        CK(cudaMallocHost(&hres_, (prow + 1) * sizeof(double)), "alloc pinned results");
+        hres_n_ = prow + 1;
     }
     return FKADJ_OK;
 }
@@ -583,15 +629,24 @@ fkadj_status Problem::autotune() {
     CK(cudaEventCreate(&a), "event");
     CK(cudaEventCreate(&b), "event");
     const double E = Et_.empty() ? 0.0 : Et_[0];
+    // one warm-up launch, then the best of three rounds of three launches
+    // (a single round mis-ranked presets whose times differ by a few percent)
     auto timed = [&](auto&& launch, float* ms) -> cudaError_t {
         cudaError_t e = launch();
         if (e) return e;
-        if ((e = cudaEventRecord(a, st_))) return e;
-        for (int r = 0; r < 3; ++r)
-            if ((e = launch())) return e;
-        if ((e = cudaEventRecord(b, st_))) return e;
-        if ((e = cudaEventSynchronize(b))) return e;
-        return cudaEventElapsedTime(ms, a, b);
+        float best = 1e30f;
+        for (int round = 0; round < 3; ++round) {
+            if ((e = cudaEventRecord(a, st_))) return e;
+            for (int r = 0; r < 3; ++r)
+                if ((e = launch())) return e;
+            if ((e = cudaEventRecord(b, st_))) return e;
+            if ((e = cudaEventSynchronize(b))) return e;
+            float t = 0;
+            if ((e = cudaEventElapsedTime(&t, a, b))) return e;
+            best = t < best ? t : best;
+        }
+        *ms = best;
+        return cudaSuccess;
     };
     // every preset at its own height; the forward step and the midpoint also
     // with the rows that fit the grid into one wave of CTAs
@@ -607,14 +662,14 @@ fkadj_status Problem::autotune() {
                 float ms = 0;
                 cudaError_t e = timed([&]() { return make_launch(t, rows[k]); }, &ms);
                 if (e) return e;
-                launches_ += 4;
+                launches_ += 10;
                 if (ms < best) best = ms, tk_[kind] = t, ty_[kind] = rows[k];
             }
         }
         return cudaSuccess;
     };
     cudaError_t e = pick(T_FWD, [&](int t, int ty) {
-        return launch_fwd_step(t, P_, g_, y, out, gh_.as<double>(), E, E, E, st_, nullptr, ty);
+        return launch_fwd_step(t, P_, g_, y, out, gh_.as<double>(), EStep::values(E, E, E), st_, nullptr, ty);
     });
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_REF) {
         double* z2 = zbuf_.as<double>() + state_elems();
@@ -623,7 +678,8 @@ fkadj_status Problem::autotune() {
         double* fc = fcache_.as<double>();
         // trial launches with the caches in use, as in the backward sweep
         e = pick(T_MID, [&](int t, int ty) {
-            return launch_adj_mid(t, P_, g_, y, y, gh_.as<double>(), yh_.as<double>(), E, E, E, hw_, st_, fc,
+            return launch_adj_mid(t, P_, g_, y, y, gh_.as<double>(), yh_.as<double>(), EStep::values(E, E, E), hw_,
+                                  st_, fc,
                                   fc + 3 * pl, jc + 14 * pl, ty);
         });
         if (!e)
@@ -634,7 +690,7 @@ fkadj_status Problem::autotune() {
     }
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_EXACT) {
         double* z2 = zbuf_.as<double>() + state_elems();
-        e = launch_fwd_step(tk_[T_FWD], P_, g_, y, out, gh_.as<double>(), E, E, E, st_, stg_.as<double>(),
+        e = launch_fwd_step(tk_[T_FWD], P_, g_, y, out, gh_.as<double>(), EStep::values(E, E, E), st_, stg_.as<double>(),
                             ty_[T_FWD]);
         if (!e)
             e = pick(T_EXACT, [&](int t, int) {
@@ -722,8 +778,7 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
     double* stg = stg_.as<double>();
     auto back = [&](int t, const double* y) -> fkadj_status {
         CK(prof_begin(K_FWD), "profiling event");
-        CK(launch_fwd_step(tk_[T_FWD], P_, g_, y, scratch, gh_.as<double>(), Et_[t], Eh_[t], Et_[t + 1], st_,
-                           stg, ty_[T_FWD]),
+        CK(launch_fwd_step(tk_[T_FWD], P_, g_, y, scratch, gh_.as<double>(), efwd(t), st_, stg, ty_[T_FWD]),
            "stage replay");
         CK(prof_end(K_FWD), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
@@ -760,33 +815,13 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
     return FKADJ_OK;
 }
 
-fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, double* LE, double* Lcost,
-                           double* gradE, double* yf) {
+fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_out) {
     fkadj_status s;
-    launches_ = 0;
-    if (!gradE) {
-        set_error("gradE is null");
-        return FKADJ_ERR_ARG;
-    }
-    if (grad_mode_ != FKADJ_GRAD_REF && grad_mode_ != FKADJ_GRAD_EXACT) {
-        set_error("unknown gradient mode");
-        return FKADJ_ERR_ARG;
-    }
-    const bool exact = grad_mode_ == FKADJ_GRAD_EXACT;
-    if ((s = prepare_E(Et))) return s;
-    TrajPlan tp;
-    if ((s = plan_trajectory(tp))) return s;
-    if ((s = ensure_traj(tp))) return s;
-    if ((s = ensure_adjoint_work())) return s;
     const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
     const size_t nsb = (size_t)nsb_;
-    CK(cudaEventRecord(ev_[0], st_), "event");
-    // ---- forward sweep, storing states (cu-G:1689-1724 without the D2H copies)
-    if ((s = upload_state(y_ini, slot(0)))) return s;
-    if (autotune_ && !tuned_) {
-        if ((s = autotune())) return s;
-        tuned_ = tuned_fwd_ = true;
-    }
+    auto record = [&](cudaEvent_t e) {
+        return capturing_ ? cudaEventRecordWithFlags(e, st_, cudaEventRecordExternal) : cudaEventRecord(e, st_);
+    };
     double* cur = slot(0);
     const bool binomial = tp.policy == FKADJ_CKPT_BINOMIAL;
     for (int i = 0; i < nt; ++i) {
@@ -801,10 +836,11 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         cur = out;
     }
     double* yT = cur;
-    CK(cudaEventRecord(ev_[1], st_), "event");
+    *yT_out = yT;
+    CK(record(ev_[1]), "event");
     // ---- objective and terminal adjoint state z(T) = -gamma S y(T) (cu-G:1769-1838)
-    double l0 = 0;
-    if ((s = run_objective(yT, &l0))) return s;
+    if ((s = objective_async(yT))) return s;
+    CK(cudaMemcpyAsync(hres_, osum_.p, sizeof(double), cudaMemcpyDeviceToHost, st_), "download L0");
     double* z = zbuf_.as<double>();
     double* z2 = z + state_elems();
     double* part = partial_.as<double>();
@@ -835,8 +871,8 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         const int nxt = 1 - cur_c;
         const double* fin = fb ? fb : (have_fcarry ? fc[cur_c] : nullptr);
         CK(prof_begin(K_MID), "profiling event");
-        CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), Et_[i - 1], Et_[i],
-                          E3_[i - 1], hw_, st_, fin, fa ? nullptr : fc[nxt], jh, ty_[T_MID], fa),
+        CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), emid(i), hw_, st_, fin,
+                          fa ? nullptr : fc[nxt], jh, ty_[T_MID], fa),
            "adjoint midpoint");
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
@@ -898,13 +934,94 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     const int rows = exact ? 3 * nt : nt + 1;
     CK(launch_sum_rows(part, rows, nsb_, zgh_.as<double>(), st_), "reduce z.gh");
     ++launches_;
-    std::vector<double> zgh(rows);
-    CK(cudaMemcpyAsync(zgh.data(), zgh_.p, rows * sizeof(double), cudaMemcpyDeviceToHost, st_),
-       "download z.gh");
-    CK(cudaEventRecord(ev_[2], st_), "event");
+    CK(cudaMemcpyAsync(hres_ + 1, zgh_.p, rows * sizeof(double), cudaMemcpyDeviceToHost, st_), "download z.gh");
+    CK(record(ev_[2]), "event");
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::grad_replay(const TrajPlan& tp, bool exact, double** yT) {
+    GraphKey key;
+    key.policy = tp.policy;
+    key.nslots = tp.nslots;
+    key.seg_slots = tp.seg_slots;
+    key.keep_f = tp.keep_f;
+    key.exact = exact;
+    key.gen = buf_gen_;
+    for (int k = 0; k < 4; ++k) key.tk[k] = tk_[k], key.ty[k] = ty_[k];
+    if (!gexec_ || !(key == gkey_)) {
+        drop_graph();
+        const int64_t before = launches_;
+        cudaError_t e = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {  // this stream cannot be captured: plain launches from now on
+            cudaGetLastError();
+            graphs_ = false;
+            return grad_sequence(tp, exact, yT);
+        }
+        capturing_ = true;
+        const fkadj_status s = grad_sequence(tp, exact, &gyT_);
+        capturing_ = false;
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamEndCapture(st_, &graph);
+        if (s != FKADJ_OK || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            if (s != FKADJ_OK) return s;
+            graphs_ = false;
+            launches_ = before;
+            return grad_sequence(tp, exact, yT);
+        }
+        e = cudaGraphInstantiate(&gexec_, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            gexec_ = nullptr;
+            cudaGetLastError();
+            graphs_ = false;
+            launches_ = before;
+            return grad_sequence(tp, exact, yT);
+        }
+        gkey_ = key;
+        glaunches_ = launches_ - before;
+        launches_ = before;
+    }
+    CK(cudaGraphLaunch(gexec_, st_), "graph launch");
+    launches_ += glaunches_;
+    *yT = gyT_;
+    return FKADJ_OK;
+}
+
+fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, double* LE, double* Lcost,
+                           double* gradE, double* yf) {
+    fkadj_status s;
+    launches_ = 0;
+    if (!gradE) {
+        set_error("gradE is null");
+        return FKADJ_ERR_ARG;
+    }
+    if (grad_mode_ != FKADJ_GRAD_REF && grad_mode_ != FKADJ_GRAD_EXACT) {
+        set_error("unknown gradient mode");
+        return FKADJ_ERR_ARG;
+    }
+    const bool exact = grad_mode_ == FKADJ_GRAD_EXACT;
+    if ((s = prepare_E(Et))) return s;
+    TrajPlan tp;
+    if ((s = plan_trajectory(tp))) return s;
+    if ((s = ensure_traj(tp))) return s;
+    if ((s = ensure_adjoint_work())) return s;
+    const int nt = nt_;
+    CK(cudaEventRecord(ev_[0], st_), "event");
+    // ---- forward sweep, storing states (cu-G:1689-1724 without the D2H copies)
+    if ((s = upload_state(y_ini, slot(0)))) return s;
+    if (autotune_ && !tuned_) {
+        if ((s = autotune())) return s;
+        tuned_ = tuned_fwd_ = true;
+    }
+    double* yT = nullptr;
+    if ((s = (graphs_ && !profiling_) ? grad_replay(tp, exact, &yT) : grad_sequence(tp, exact, &yT))) return s;
     if (yf && (s = download_grid(yT, yf))) return s;
     CK(cudaStreamSynchronize(st_), "synchronize");
     if ((s = prof_collect())) return s;
+    const double l0 = -hres_[0];
+    const double* zgh = hres_ + 1;
     double le = 0;
     for (int i = 0; i <= nt; ++i) le += Et_[i] * Et_[i];
     le *= dt_;
@@ -917,7 +1034,7 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
             gE[t] += zgh[t];
             gE[t + 1] += zgh[2 * nt + t];
         }
-        spline_->transpose_add(0.5, zgh.data() + nt, gE.data());
+        spline_->transpose_add(0.5, zgh + nt, gE.data());
         for (int i = 0; i <= nt; ++i) gradE[i] = (gE[i] + alpha_ * dt_ * Et_[i]) / dt_;
     } else {
         for (int i = 0; i <= nt; ++i) gradE[i] = alpha_ * Et_[i] - zgh[i];  // cu-G:1924-1926

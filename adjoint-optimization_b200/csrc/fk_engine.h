@@ -109,7 +109,9 @@ public:
     // upload_state with y_ini == nullptr re-uses the initial state of the
     // previous call (kept resident on the device).
     fkadj_status upload_state(const double* y_ini, double* d_state);
-    fkadj_status prepare_E(const double* Et);
+    // Spline samples of Et on the host; with upload, also the device tables the
+    // standalone kernels read (the batched kernels take E by value).
+    fkadj_status prepare_E(const double* Et, bool upload = true);
     fkadj_status step_forward(int i, const double* yin, double* yout, double* k1 = nullptr);
     double* state_buf(int k) const { return work_.as<double>() + (size_t)k * state_elems(); }
     size_t state_elems() const { return (size_t)3 * g_.plane; }
@@ -134,6 +136,23 @@ private:
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
     double* segslot(int k) const { return seg_.as<double>() + (size_t)k * state_elems(); }
     double* fslot(int k) const { return kf_.as<double>() + (size_t)k * state_elems(); }
+    // E samples of step i read from the device tables (uploaded by prepare_E)
+    const double* etab() const { return Ed_.as<double>(); }
+    EStep efwd(int i) const {
+        const double* t = etab();
+        return EStep::table(t + i, t + (nt_ + 1) + i, t + i + 1);  // Et[i], E(t_i + dt/2), Et[i+1]
+    }
+    EStep emid(int i) const {
+        const double* t = etab();
+        return EStep::table(t + i - 1, t + i, t + (2 * nt_ + 1) + i - 1);  // Et[i-1], Et[i], E(t_{i-1} + dt/3)
+    }
+    // The gradient's device work after the initial state is in place: forward
+    // sweep, objective, backward sweep, reductions, and the copies of L0 and the
+    // z.gh rows into pinned host memory.  Issued directly or captured once into a
+    // CUDA graph and replayed (use_graph).
+    fkadj_status grad_sequence(const TrajPlan& tp, bool exact, double** yT);
+    fkadj_status grad_replay(const TrajPlan& tp, bool exact, double** yT);
+    void drop_graph();
 
     fkadj_params p_{};
     DevModel P_{};
@@ -163,7 +182,25 @@ private:
     DevBuf stg_;       // stage states Y2, Y3, Y4 of one step (exact mode)
     DevBuf jcache_;    // cached Jacobians (reference mode): J(y) ping-pong + J(yh)
     DevBuf fcache_;    // f(y) carried between backward steps (reference mode)
+    DevBuf Ed_;        // E tables: Et (nt+1), E at half steps (nt), E at third steps (nt)
+    double* Ehost_ = nullptr;  // pinned staging of the E tables
+    double* hres_ = nullptr;   // pinned results: L0 partial sum, then the z.gh rows
+    size_t hres_n_ = 0;
     bool have_y0_ = false;
+
+    // captured gradient sequence
+    struct GraphKey {
+        int policy = -1, nslots = 0, seg_slots = 0, keep_f = 0, exact = 0, gen = 0;
+        int tk[4] = {0, 0, 0, 0}, ty[4] = {0, 0, 0, 0};
+        bool operator==(const GraphKey& o) const;
+    };
+    bool graphs_ = true;         // FKADJ_NO_GRAPHS=1 in the environment turns replay off
+    cudaGraphExec_t gexec_ = nullptr;
+    GraphKey gkey_{};
+    int64_t glaunches_ = 0;
+    double* gyT_ = nullptr;
+    int buf_gen_ = 0;            // bumped whenever a buffer the sequence uses is reallocated
+    bool capturing_ = false;
     TrajPlan traj_plan_{};
 
     // sampled kernel timing

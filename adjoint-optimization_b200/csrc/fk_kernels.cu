@@ -216,9 +216,9 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin, double* __restrict__ yout,
-               const double* __restrict__ gh, double E0, double Eh, double E1, double* __restrict__ stages, int ty,
+               const double* __restrict__ gh, EStep E, double* __restrict__ stages, int ty,
                double* __restrict__ k1) {
-    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E0, Eh, E1, stages, blockIdx.x, blockIdx.y, ty, k1);
+    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -342,10 +342,11 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya, const double* __restrict__ yb,
-              const double* __restrict__ gh, double* __restrict__ yh, double Ea, double Eb, double E3, HermiteW hw,
+              const double* __restrict__ gh, double* __restrict__ yh, EStep E, HermiteW hw,
               const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty,
               const double* __restrict__ fa) {
-    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, blockIdx.x, blockIdx.y, ty, fa);
+    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, E.a(), E.b(), E.c(), hw, fin, fout, jh, blockIdx.x, blockIdx.y,
+                             ty, fa);
 }
 
 // One adjoint stage on the tile grown by E cells: k = L^T src + J_F(y)^T src,
@@ -832,12 +833,11 @@ static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
 }
 
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
-                            const double* gh, double E0, double Eh, double E1, cudaStream_t st,
-                            double* stages, int ty, double* k1) {
+                            const double* gh, const EStep& E, cudaStream_t st, double* stages, int ty, double* k1) {
     DISPATCH(tile, {
         const int rows = (ty > 0 && ty < TY) ? ty : TY;
         k_fwd_step<TX, TY, NT><<<tile_grid(g, TX, rows), NT, stencil_smem<TX, TY>(NT), st>>>(
-            P, g, yin, yout, gh, E0, Eh, E1, stages, rows, k1);
+            P, g, yin, yout, gh, E, stages, rows, k1);
     });
     return cudaGetLastError();
 }
@@ -851,13 +851,12 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
 }
 
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
-                           const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
-                           cudaStream_t st, const double* fin, double* fout, double* jh, int ty,
-                           const double* fa) {
+                           const double* gh, double* yh, const EStep& E, const HermiteW& hw, cudaStream_t st,
+                           const double* fin, double* fout, double* jh, int ty, const double* fa) {
     DISPATCH(tile, {
         const int rows = (ty > 0 && ty < TY) ? ty : TY;
         k_adj_mid<TX, TY, NT><<<tile_grid(g, TX, rows), NT, mid_smem<TX, TY>(), st>>>(
-            P, g, ya, yb, gh, yh, Ea, Eb, E3, hw, fin, fout, jh, rows, fa);
+            P, g, ya, yb, gh, yh, E, hw, fin, fout, jh, rows, fa);
     });
     return cudaGetLastError();
 }

@@ -38,6 +38,23 @@ enum BatchKind { BATCH_FWD = 0, BATCH_MID = 1, BATCH_ADJ_REF = 2, BATCH_ADJ_EXAC
 //              fin/fout (f carry), jh (J(yh) out)
 //   ADJ_REF    a = z, out = z_out, b = y_i, c = yh, d = y_{i-1}, row, jb/jh/ja (J caches)
 //   ADJ_EXACT  a = lambda, out = lambda_out, b = y_s, stages, row/row2/row3
+// The three E samples of one step: (E0, Eh, E1) = (Et[i], E(t_i + dt/2),
+// Et[i+1]) for the forward step, (Ea, Eb, E3) = (Et[i-1], Et[i], E(t_{i-1} +
+// dt/3)) for the adjoint midpoint.  Either by value, or read by the kernel from
+// device tables (p[k] non-null), so a captured launch sequence (CUDA graph)
+// replays with new samples written into the tables.
+struct EStep {
+    double v[3];
+    const double* p[3];
+    __host__ __device__ static EStep values(double a, double b, double c) { return {{a, b, c}, {nullptr, nullptr, nullptr}}; }
+    __host__ __device__ static EStep table(const double* a, const double* b, const double* c) {
+        return {{0.0, 0.0, 0.0}, {a, b, c}};
+    }
+    __device__ double a() const { return p[0] ? *p[0] : v[0]; }
+    __device__ double b() const { return p[1] ? *p[1] : v[1]; }
+    __device__ double c() const { return p[2] ? *p[2] : v[2]; }
+};
+
 struct BatchItem {
     int inst, tile0, ntx, kind;
     const double *a, *b, *c, *d;
@@ -74,8 +91,8 @@ cudaError_t kernels_init();
 // k1 = f(y, E0) is kept (a state, null = not kept).  fa (midpoint): f(ya, Ea)
 // as kept by the forward step from ya (null = evaluate).
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
-                            const double* gh, double E0, double Eh, double E1, cudaStream_t st,
-                            double* stages = nullptr, int ty = 0, double* k1 = nullptr);
+                            const double* gh, const EStep& E, cudaStream_t st, double* stages = nullptr, int ty = 0,
+                            double* k1 = nullptr);
 // Rows per tile that fit grid g into one wave of CTAs of preset `tile` for
 // kernel kind 0 (forward step) or 1 (adjoint midpoint); the preset's height
 // when it does not fit.
@@ -88,9 +105,9 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
                              const double* y, const double* stages, const uint8_t* wc, const double* gh,
                              double* r1, double* r23, double* r4, int nsbx, cudaStream_t st);
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
-                           const double* gh, double* yh, double Ea, double Eb, double E3, const HermiteW& hw,
-                           cudaStream_t st, const double* fin = nullptr, double* fout = nullptr,
-                           double* jh = nullptr, int ty = 0, const double* fa = nullptr);
+                           const double* gh, double* yh, const EStep& E, const HermiteW& hw, cudaStream_t st,
+                           const double* fin = nullptr, double* fout = nullptr, double* jh = nullptr, int ty = 0,
+                           const double* fa = nullptr);
 // jb: cached J(y_i) (null = evaluate), jh: cached J(yh) (null = evaluate),
 // ja: where J(y_{i-1}) is stored for the next step (null = not kept).
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,

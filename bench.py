@@ -50,8 +50,10 @@ BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
                   2: 249.0}   # adjoint step: read z (24) + J(y_i), J(yh) (112) + y_{i-1} (24) + gh (8)
                               #   + weight code (1), write z (24) + J(y_{i-1}) (56)
 # DRAM bytes per cell of one k_fwd_step launch measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, cold L2) at 512x512: profiles/k_fwd_step_512x512_traffic.md
-FWD_TRAFFIC_PER_CELL = None
+# dram__bytes_write.sum, caches flushed before the launch) at 512x512:
+# profiles/k_fwd_step_512x512_traffic.md.  The reads (33 B/cell: y 24 + gh 8 +
+# halo) reach DRAM; the 24 B/cell of writes stay in the 126 MB L2.
+FWD_TRAFFIC_PER_CELL = 8656640 / 262144
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
 
 
