@@ -939,7 +939,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
     return FKADJ_OK;
 }
 
-fkadj_status Problem::grad_replay(const TrajPlan& tp, bool exact, double** yT) {
+Problem::GraphKey Problem::graph_key(const TrajPlan& tp, bool exact) const {
     GraphKey key;
     key.policy = tp.policy;
     key.nslots = tp.nslots;
@@ -948,6 +948,11 @@ fkadj_status Problem::grad_replay(const TrajPlan& tp, bool exact, double** yT) {
     key.exact = exact;
     key.gen = buf_gen_;
     for (int k = 0; k < 4; ++k) key.tk[k] = tk_[k], key.ty[k] = ty_[k];
+    return key;
+}
+
+fkadj_status Problem::grad_replay(const TrajPlan& tp, bool exact, double** yT) {
+    const GraphKey key = graph_key(tp, exact);
     if (!gexec_ || !(key == gkey_)) {
         drop_graph();
         const int64_t before = launches_;
@@ -1015,8 +1020,14 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         if ((s = autotune())) return s;
         tuned_ = tuned_fwd_ = true;
     }
+    // A configuration's first gradient runs as plain launches; from its second
+    // on, the sequence is captured once and replayed (a one-shot call, such as
+    // the drop-in fkadj_grad, never pays for capture and instantiation).
     double* yT = nullptr;
-    if ((s = (graphs_ && !profiling_) ? grad_replay(tp, exact, &yT) : grad_sequence(tp, exact, &yT))) return s;
+    const GraphKey key = graph_key(tp, exact);
+    const bool replay = graphs_ && !profiling_ && ((gexec_ && key == gkey_) || key == seen_key_);
+    seen_key_ = key;
+    if ((s = replay ? grad_replay(tp, exact, &yT) : grad_sequence(tp, exact, &yT))) return s;
     if (yf && (s = download_grid(yT, yf))) return s;
     CK(cudaStreamSynchronize(st_), "synchronize");
     if ((s = prof_collect())) return s;

@@ -197,6 +197,8 @@ private:
     bool graphs_ = true;         // FKADJ_NO_GRAPHS=1 in the environment turns replay off
     cudaGraphExec_t gexec_ = nullptr;
     GraphKey gkey_{};
+    GraphKey seen_key_{};        // configuration of the previous gradient
+    GraphKey graph_key(const TrajPlan& tp, bool exact) const;
     int64_t glaunches_ = 0;
     double* gyT_ = nullptr;
     int buf_gen_ = 0;            // bumped whenever a buffer the sequence uses is reallocated

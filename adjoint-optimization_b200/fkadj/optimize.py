@@ -49,19 +49,25 @@ def interval_gradient(gradE_exact, dt, interval_of_sample, K):
 
 
 def armijo_descent(inst, iters: int, probes: int = 6, s0: float | None = None, beta: float = 0.5,
-                   c1: float = 1e-4, amplitudes=None, grow: float = 2.0):
-    """Returns dict(A, J (per iteration, at the iterate), step, evals) ."""
+                   c1: float = 1e-4, amplitudes=None, grow: float = 2.0, ckpt_policy: int = _lib.CKPT_AUTO,
+                   ckpt_budget_bytes: int = 0):
+    """Returns dict(A, J (per iteration, at the iterate), step, armijo_ok,
+    probes, t_grad / t_probes: wall seconds per iteration of the gradient and
+    of the probe batch, device_bytes of the gradient problem)."""
+    import time
     K = len(inst.amplitudes)
     A = np.array(inst.amplitudes if amplitudes is None else amplitudes, dtype=np.float64)
     nt = inst.nt
-    hist = {"J": [], "step": [], "armijo_ok": [], "probes": []}
-    gopts = api.options(grad_mode=_lib.GRAD_EXACT)
+    hist = {"J": [], "step": [], "armijo_ok": [], "probes": [], "t_grad": [], "t_probes": []}
+    gopts = api.options(grad_mode=_lib.GRAD_EXACT, ckpt_policy=ckpt_policy, ckpt_budget_bytes=ckpt_budget_bytes)
     with api.Problem(inst, opts=gopts) as pb, Batch() as bt:
         pids = [bt.add_problem(inst) for _ in range(probes)]
         first = True
         for it in range(iters):
             E = piecewise_constant(nt, A)[0]
+            t0 = time.perf_counter()
             r = pb.grad(E, inst.y0 if first else None)
+            hist["t_grad"].append(time.perf_counter() - t0)
             first = False
             J0 = r["Lcost"]
             g = interval_gradient(r["gradE"], inst.dt, inst.interval_of_sample, K)
@@ -70,10 +76,12 @@ def armijo_descent(inst, iters: int, probes: int = 6, s0: float | None = None, b
             if s0 is None:
                 s0 = 0.1 * max(1.0, np.abs(A).max()) / max(np.abs(d).max(), 1e-300)
             steps = [s0 * beta ** k for k in range(probes)]
+            t0 = time.perf_counter()
             jobs = [bt.submit(p, piecewise_constant(nt, A + s * d)[0], inst.y0, want_grad=False)
                     for p, s in zip(pids, steps)]
             bt.run()
             Js = [bt.result(j)["Lcost"] for j in jobs]
+            hist["t_probes"].append(time.perf_counter() - t0)
             ok = [Jk <= J0 + c1 * s * slope for Jk, s in zip(Js, steps)]
             hist["J"].append(J0)
             hist["probes"].append(list(zip(steps, Js)))
@@ -87,5 +95,6 @@ def armijo_descent(inst, iters: int, probes: int = 6, s0: float | None = None, b
                 hist["step"].append(0.0)
                 hist["armijo_ok"].append(False)
                 s0 = steps[-1] * beta
+        device_bytes = pb.device_bytes
     return dict(A=A, J=np.array(hist["J"]), step=np.array(hist["step"]), armijo_ok=hist["armijo_ok"],
-                probes=hist["probes"])
+                probes=hist["probes"], t_grad=hist["t_grad"], t_probes=hist["t_probes"], device_bytes=device_bytes)

@@ -12,6 +12,12 @@
       above: served latency p50/p99 and throughput, against the same stream
       solved one request at a time (FIFO, each request's standalone time)
 
+  python -m fkadj.suite opt   [--n 2048 --nt 100000 --iters 1 --probes 4 --budget-gb 60]
+      the optimisation loop at scale: Armijo descent on the interval
+      amplitudes of the energy-penalised cost (discrete-exact gradient,
+      checkpoints chosen within the HBM budget: binomial at 2048^2 x 1e5),
+      trial steps batched; time per gradient and per probe batch, J history
+
 Sizes can be scaled down (max side, horizon scale) to fit a time budget; the
 line says which.  Inputs are seeded synthetic instances (fkadj.workloads).
 """
@@ -134,6 +140,20 @@ def cmd_serve(a):
                           "peak_running": peak}), flush=True)
 
 
+def cmd_opt(a):
+    from .optimize import armijo_descent
+    inst = W.scale_instance(n=a.n, nt=a.nt, alpha=a.alpha)
+    t0 = time.perf_counter()
+    out = armijo_descent(inst, iters=a.iters, probes=a.probes, ckpt_budget_bytes=int(a.budget_gb * 1e9))
+    wall = time.perf_counter() - t0
+    state = 3 * (a.n + 72) * (a.n + 72) * 8
+    print(json.dumps({"suite": "opt", "grid": a.n, "nt": a.nt, "holes": 3000, "wavefronts": 32, "intervals": 1000,
+                      "alpha": a.alpha, "iters": a.iters, "probes": a.probes, "budget_gb": a.budget_gb,
+                      "full_store_gb": (a.nt + 1) * state / 1e9, "device_bytes": out["device_bytes"],
+                      "J": out["J"].tolist(), "step": out["step"].tolist(), "armijo_ok": out["armijo_ok"],
+                      "t_grad_s": out["t_grad"], "t_probes_s": out["t_probes"], "wall_s": wall}), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="fkadj.suite")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -154,8 +174,15 @@ def main(argv=None):
         else:
             p.add_argument("--requests", type=int, default=48)
             p.add_argument("--rates", type=lambda s: [float(x) for x in s.split(",")], default=[10, 50, 200, 500])
+    o = sub.add_parser("opt")
+    o.add_argument("--n", type=int, default=2048)
+    o.add_argument("--nt", type=int, default=100000)
+    o.add_argument("--iters", type=int, default=1)
+    o.add_argument("--probes", type=int, default=4)
+    o.add_argument("--budget-gb", type=float, default=60.0)
+    o.add_argument("--alpha", type=float, default=0.05)
     a = ap.parse_args(argv)
-    {"ckpt": cmd_ckpt, "batch": cmd_batch, "serve": cmd_serve}[a.cmd](a)
+    {"ckpt": cmd_ckpt, "batch": cmd_batch, "serve": cmd_serve, "opt": cmd_opt}[a.cmd](a)
 
 
 if __name__ == "__main__":

@@ -55,6 +55,21 @@ BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
 # halo) reach DRAM; the 24 B/cell of writes stay in the 126 MB L2.
 FWD_TRAFFIC_PER_CELL = 8656640 / 262144
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
+# FP64 flops per vector-field evaluation of the forward step (stage update included), counted by ncu
+# (2 x DFMA + DMUL + DADD thread instructions): profiles/fp64_ops_512x512.md
+FWD_FLOPS_PER_EVAL = 904.1 / 5.234375
+
+
+def fwd_evaluations(nrows, ncols, tx, ty):
+    """Vector-field evaluations of one forward-step launch: stage s of a tile
+    runs on the tile grown by 4 - s cells (temporal blocking); bottom-row tiles
+    stop at the grid's edge."""
+    n = 0
+    for i0 in range(0, nrows, ty):
+        rows = min(ty, nrows - i0)
+        per = sum((tx + 2 * e) * (rows + 2 * e) for e in range(4))
+        n += per * ((ncols + tx - 1) // tx)
+    return n
 
 
 def peaks():
@@ -241,6 +256,15 @@ def run_ours(args):
             "note": "FP64 bound: a vector-field evaluation costs 2 exp, 3 reciprocals, 1 divide and ~60 "
                     "FMA-class operations, 4.6 evaluations per cell-step; the HBM fraction is reported "
                     "against the copy peak"}
+    # the forward step against the FP64 roof (the bound it is nearer to)
+    ftx, fty, _ = tiles["fwd_step"]
+    fl = FWD_FLOPS_PER_EVAL * fwd_evaluations(inst.nrows, inst.ncols, ftx, fty)
+    mhz = clocks.get("sm_mhz") or 1965.0
+    fpeak = 148 * 128 * mhz * 1e6 / 1e12
+    roof["fp64"] = {"kernel": "k_fwd_step", "achieved": fl / (kt[0][0] / 1000.0) / 1e12, "peak": fpeak,
+                    "unit": "TFLOP/s", "frac": fl / (kt[0][0] / 1000.0) / 1e12 / fpeak,
+                    "flops_per_launch": fl, "peak_source": "148 SMs x 64 DFMA/clock x 2 at the sampled SM clock",
+                    "flops_source": "ncu-counted FP64 instructions per evaluation, profiles/fp64_ops_512x512.md"}
     if roof["traffic"] is None and dom == 0 and FWD_TRAFFIC_PER_CELL:
         roof["traffic"] = FWD_TRAFFIC_PER_CELL * cells
         roof["traffic_source"] = "ncu capture, profiles/k_fwd_step_512x512_traffic.md"
