@@ -204,7 +204,7 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
         }
         j->tp.keep_f = false;  // the batched midpoint evaluates f itself
         if ((s = P.ensure_traj(j->tp))) return s;
-        if ((s = P.ensure_adjoint_work())) return s;
+        if ((s = P.ensure_adjoint_work(true))) return s;  // the batch reduces all rows at the end
         if ((s = P.upload_state(y_ini, P.slot(0)))) return s;
         j->cur = P.slot(0);
         j->z = P.zbuf_.as<double>();

@@ -587,7 +587,7 @@ fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
     return FKADJ_OK;
 }
 
-fkadj_status Problem::ensure_adjoint_work() {
+fkadj_status Problem::ensure_adjoint_work(bool all_rows) {
     if (!zbuf_.p) {
         CK(zbuf_.alloc(2 * state_bytes()), "alloc adjoint states");
         CK(cudaMemsetAsync(zbuf_.p, 0xff, zbuf_.bytes, st_), "init adjoint states");
@@ -605,11 +605,24 @@ fkadj_status Problem::ensure_adjoint_work() {
         CK(stg_.alloc(3 * state_bytes()), "alloc stage states");
         CK(cudaMemsetAsync(stg_.p, 0xff, stg_.bytes, st_), "init stage states");
     }
-    const size_t prow = (size_t)(3 * nt_ + 1);  // exact mode keeps 3 rows per step
-    const size_t pbytes = prow * (size_t)nsb_ * sizeof(double);
-    if (partial_.bytes < pbytes) {
+    // z.gh partials, one row of nsb sub-block sums per row of results.  The
+    // standalone sweep keeps a window of kPartialWindow rows per group (the
+    // exact mode has three groups of nt rows, the reference mode one of nt+1)
+    // and reduces each block of rows as soon as the backward sweep, which
+    // visits rows in decreasing order, has written its lowest one; the batch
+    // engine keeps every row.
+    const size_t prow = (size_t)(3 * nt_ + 1);
+    const int groups = grad_mode_ == FKADJ_GRAD_EXACT ? 3 : 1;
+    const int per_group = grad_mode_ == FKADJ_GRAD_EXACT ? nt_ : nt_ + 1;
+    const int win = all_rows ? (int)prow : std::min(per_group, kPartialWindow);
+    const size_t pbytes = (all_rows ? prow : (size_t)groups * win) * (size_t)nsb_ * sizeof(double);
+    if (partial_.bytes < pbytes || pwin_ != win) {
         CK(partial_.alloc(pbytes), "alloc partials");
         CK(cudaMemsetAsync(partial_.p, 0, partial_.bytes, st_), "zero partials");
+        pwin_ = win;
+        ++buf_gen_;
+    }
+    if (zgh_.bytes < prow * sizeof(double)) {
         CK(zgh_.alloc(prow * sizeof(double)), "alloc zgh");
         ++buf_gen_;
     }
@@ -769,11 +782,6 @@ fkadj_status Problem::reverse_binomial(int a, int b, double* ya, std::vector<dou
 fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2) {
     fkadj_status s;
     const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
-    const size_t nsb = (size_t)nsb_;
-    double* part = partial_.as<double>();
-    double* p1 = part;
-    double* p23 = part + (size_t)nt * nsb;
-    double* p4 = part + 2 * (size_t)nt * nsb;
     double* scratch = state_buf(1);
     double* stg = stg_.as<double>();
     auto back = [&](int t, const double* y) -> fkadj_status {
@@ -783,11 +791,13 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
         CK(prof_end(K_FWD), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_exact(tk_[T_EXACT], P_, g_, lam, lam2, y, stg, wc_.as<uint8_t>(), gh_.as<double>(),
-                            p1 + t * nsb, p23 + t * nsb, p4 + t * nsb, nsbx_, st_),
+                            prow(0, t), prow(1, t), prow(2, t), nsbx_, st_),
            "exact adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
         std::swap(lam, lam2);
+        if (t % pwin_ == 0)  // rows t .. t+pwin-1 of the three groups are complete
+            for (int g = 0; g < 3; ++g) CK(flush_rows(g, t, nt), "reduce z.gh");
         return FKADJ_OK;
     };
     if (tp.policy == FKADJ_CKPT_FULL) {
@@ -815,10 +825,16 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
     return FKADJ_OK;
 }
 
+cudaError_t Problem::flush_rows(int g, int row, int rows_g) {
+    ++launches_;
+    const int n = std::min(pwin_, rows_g - row);
+    return launch_sum_rows(partial_.as<double>() + (size_t)g * pwin_ * nsb_, n, nsb_,
+                           zgh_.as<double>() + (size_t)g * nt_ + row, st_);
+}
+
 fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_out) {
     fkadj_status s;
     const int nt = nt_, c = tp.stride, K = tp.nslots - 1;
-    const size_t nsb = (size_t)nsb_;
     auto record = [&](cudaEvent_t e) {
         return capturing_ ? cudaEventRecordWithFlags(e, st_, cudaEventRecordExternal) : cudaEventRecord(e, st_);
     };
@@ -843,7 +859,6 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
     CK(cudaMemcpyAsync(hres_, osum_.p, sizeof(double), cudaMemcpyDeviceToHost, st_), "download L0");
     double* z = zbuf_.as<double>();
     double* z2 = z + state_elems();
-    double* part = partial_.as<double>();
     if (exact) {
         // lambda(T) = dJ/dy(T) = -z(T); discrete adjoint sweep
         CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), -1.0, z, st_), "scatter lambda");
@@ -851,8 +866,9 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         if ((s = grad_exact_backward(tp, z, z2))) return s;
     } else {
         CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, z, st_), "scatter z");
-        CK(launch_dot_gh(g_, z, gh_.as<double>(), part + (size_t)nt * nsb, nsbx_, nsby_, st_), "z.gh");
+        CK(launch_dot_gh(g_, z, gh_.as<double>(), prow(0, nt), nsbx_, nsby_, st_), "z.gh");
         launches_ += 2;
+        if (nt % pwin_ == 0) CK(flush_rows(0, nt, nt + 1), "reduce z.gh");
     }
     // ---- backward sweep (cu-G:1866-1908)
     // Work carried from backward step i to step i-1 (computed once, same
@@ -877,11 +893,12 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
-                           gh_.as<double>(), part + (size_t)(i - 1) * nsb, nsbx_, st_,
+                           gh_.as<double>(), prow(0, i - 1), nsbx_, st_,
                            have_jcarry ? jy[cur_c] : nullptr, jh, jy[nxt]),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
+        if ((i - 1) % pwin_ == 0) CK(flush_rows(0, i - 1, nt + 1), "reduce z.gh");
         std::swap(z, z2);
         cur_c = nxt;
         have_fcarry = fa == nullptr;
@@ -932,8 +949,6 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         }
     }
     const int rows = exact ? 3 * nt : nt + 1;
-    CK(launch_sum_rows(part, rows, nsb_, zgh_.as<double>(), st_), "reduce z.gh");
-    ++launches_;
     CK(cudaMemcpyAsync(hres_ + 1, zgh_.p, rows * sizeof(double), cudaMemcpyDeviceToHost, st_), "download z.gh");
     CK(record(ev_[2]), "event");
     return FKADJ_OK;
@@ -963,7 +978,9 @@ fkadj_status Problem::grad_replay(const TrajPlan& tp, bool exact, double** yT) {
             return grad_sequence(tp, exact, yT);
         }
         capturing_ = true;
+        set_launch_pdl(false);
         const fkadj_status s = grad_sequence(tp, exact, &gyT_);
+        set_launch_pdl(true);
         capturing_ = false;
         cudaGraph_t graph = nullptr;
         e = cudaStreamEndCapture(st_, &graph);

@@ -131,7 +131,17 @@ private:
     fkadj_status advance(int a, int m, const double* src, double* dst);
     fkadj_status reverse_binomial(int a, int b, double* ya, std::vector<double*>& free,
                                   const std::function<fkadj_status(int, const double*)>& visit);
-    fkadj_status ensure_adjoint_work();
+    // all_rows: keep the z.gh partials of every step (the batch engine);
+    // otherwise a window of kPartialWindow rows reduced as the sweep goes.
+    fkadj_status ensure_adjoint_work(bool all_rows = false);
+    // z.gh partial row `row` of group g (exact mode: 3 groups of nt rows;
+    // reference mode: one group of nt+1 rows) in the window
+    double* prow(int g, int row) const {
+        return partial_.as<double>() + ((size_t)g * pwin_ + (size_t)(row % pwin_)) * nsb_;
+    }
+    // reduces the rows row .. row+pwin-1 (clipped to rows_g) of group g into zgh
+    cudaError_t flush_rows(int g, int row, int rows_g);
+    static constexpr int kPartialWindow = 512;
     fkadj_status download_grid(const double* d_state, double* host_dense);
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
     double* segslot(int k) const { return seg_.as<double>() + (size_t)k * state_elems(); }
@@ -201,7 +211,8 @@ private:
     GraphKey graph_key(const TrajPlan& tp, bool exact) const;
     int64_t glaunches_ = 0;
     double* gyT_ = nullptr;
-    int buf_gen_ = 0;            // bumped whenever a buffer the sequence uses is reallocated
+    int buf_gen_ = 0;
+    int pwin_ = 1;               // rows per group in the z.gh partial window            // bumped whenever a buffer the sequence uses is reallocated
     bool capturing_ = false;
     TrajPlan traj_plan_{};
 

@@ -93,6 +93,9 @@ cudaError_t kernels_init();
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, const EStep& E, cudaStream_t st, double* stages = nullptr, int ty = 0,
                             double* k1 = nullptr);
+// Programmatic dependent launch for the step kernels issued by this thread
+// (on by default; the engine turns it off while it captures a graph).
+void set_launch_pdl(bool on);
 // Rows per tile that fit grid g into one wave of CTAs of preset `tile` for
 // kernel kind 0 (forward step) or 1 (adjoint midpoint); the preset's height
 // when it does not fit.

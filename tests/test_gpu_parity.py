@@ -190,3 +190,25 @@ def test_binomial_checkpointing_equals_full_storage(mode, slots):
                                            ckpt_budget_bytes=budget))
     assert np.array_equal(full[0], bino[0])
     assert full[1] == bino[1]
+
+
+@pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
+def test_windowed_zgh_reduction_matches_oracle_and_batch(mode):
+    """1300 steps: the standalone sweep reduces its z.gh partials in blocks of
+    rows as it goes (three blocks here); the batch engine keeps every row and
+    reduces once.  The two agree to 1e-12 (the batch tests' bound), and the
+    oracle within 1e-8."""
+    from fkadj.batch import Batch
+    inst = _inst(48, 1300, seed=33, ncols=64, objective="gradient", alpha=0.1)
+    g, Lc, _, _, _ = api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                                    inst.ghost, inst.gamma, inst.S, inst.alpha, params=inst.params,
+                                    opts=api.options(grad_mode=mode))
+    with Batch() as b:
+        p = b.add_problem(inst, grad_mode=mode)
+        r = b.result((b.submit(p, inst.Et, inst.y0), b.run())[0])
+    assert np.linalg.norm(r["gradE"] - g) <= 1e-12 * np.linalg.norm(g)
+    assert abs(r["Lcost"] - Lc) <= 1e-12 * abs(Lc)
+    o = O.grad(inst.params, inst.dt, inst.Et, inst.nt, inst.nrows, inst.ncols, inst.y0_grid, inst.gh_grid,
+               inst.active_index, O.Objective(inst.S, inst.gamma), inst.alpha,
+               mode="ref" if mode == _lib.GRAD_REF else "exact")
+    assert np.linalg.norm(g - o["gradE"]) <= 1e-8 * np.linalg.norm(o["gradE"])
