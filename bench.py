@@ -180,31 +180,57 @@ def run_reference(args):
     return 0
 
 
+class Ranks:
+    """One process per GPU (torchrun environment): instances are replicas, so
+    the only collectives are the barrier around the timed region and the max
+    of the per-rank times.  backend "nccl" on GPUs, "gloo" for the CPU tests."""
+
+    def __init__(self, backend="nccl", timeout_s=300):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def gmax(self, x):
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def replica_value(world, steps, ms_max):
+    """Whole-job throughput: every rank runs `steps` gradients of its own
+    replica; the job takes the slowest rank's time."""
+    return world * steps / (ms_max / 1000.0)
+
+
 def run_ours(args):
     import numpy as np
     import torch
     from fkadj import _lib, api
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ranks = Ranks("nccl")
+    rank, world, local = ranks.rank, ranks.world, ranks.local
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def gmax(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, gmax = ranks.barrier, ranks.gmax
 
     inst = workload(args)
     ckpt = {"sqrt": _lib.CKPT_SQRT, "full": _lib.CKPT_FULL, "auto": _lib.CKPT_AUTO}[args.ckpt]
@@ -230,7 +256,7 @@ def run_ours(args):
     clocks = clk.stop()
     barrier()
     ms = gmax(ev0.elapsed_time(ev1))
-    value = world * args.steps / (ms / 1000.0)
+    value = replica_value(world, args.steps, ms)
 
     # roofline: sampled per-kernel device times in one more gradient
     pb.set_profiling(True)
@@ -309,7 +335,7 @@ def run_ours(args):
                        inst.alpha, params=inst.params, opts=eopts)
     torch.cuda.synchronize()
     e2e_s = gmax(time.perf_counter() - t0)
-    e2e = {"value": world * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+    e2e = {"value": replica_value(world, e2e_steps, e2e_s * 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
            "path": "fkadj_grad (drop-in for fk_grad_Et_comp), one call per gradient incl. device setup"}
 
@@ -325,9 +351,7 @@ def run_ours(args):
         if full is not None:
             line["full_storage"] = full
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
