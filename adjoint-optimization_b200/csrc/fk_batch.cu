@@ -202,7 +202,9 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
                       "standalone engine (raise ckpt_budget_bytes or use fkadj_problem_grad)");
             return FKADJ_ERR_NOMEM;
         }
-        j->tp.keep_f = false;  // the batched midpoint evaluates f itself
+        // k1 = f(y) kept by the segment recompute (sqrt store, reference mode);
+        // the full store evaluates it (keeping it there doubles the store)
+        if (j->tp.policy != FKADJ_CKPT_SQRT) j->tp.keep_f = false;
         if ((s = P.ensure_traj(j->tp))) return s;
         if ((s = P.ensure_adjoint_work(true))) return s;  // the batch reduces all rows at the end
         if ((s = P.upload_state(y_ini, P.slot(0)))) return s;
@@ -280,6 +282,12 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
         if (t == s1) return P.slot(k + 1);
         return P.segslot(t - s0 - 1);
     };
+    // k1 = f(y_t) kept by segment k's recompute, for t = s0 .. s1-2
+    auto kept = [&](int t, int k) -> double* {
+        if (full || !j.tp.keep_f) return nullptr;
+        const int s0 = k * c, s1 = std::min(s0 + c, nt);
+        return (t >= s0 && t <= s1 - 2) ? P.fslot(t - s0) : nullptr;
+    };
     auto push = [&](BatchTick* T, BatchItem it) {
         int ntx = 1;
         const int n = ntiles(T, ntx);
@@ -315,6 +323,7 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
             it.kind = BATCH_FWD;
             it.a = seg(t, k);
             it.out = seg(t + 1, k);
+            it.k1 = kept(t, k);
             it.E0 = P.Et_[t];
             it.E1 = P.Eh_[t];
             it.E2 = P.Et_[t + 1];
@@ -338,8 +347,11 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
             m.E0 = P.Et_[i - 1];
             m.E1 = P.Et_[i];
             m.E2 = P.E3_[i - 1];
-            m.fin = j.have_carry ? fc[j.cur_c] : nullptr;
-            m.fout = fc[nxt];
+            const double* fa = kept(i - 1, k);
+            const double* fb = kept(i, k);
+            m.fa = fa;
+            m.fin = fb ? fb : (j.have_fcarry ? fc[j.cur_c] : nullptr);
+            m.fout = fa ? nullptr : fc[nxt];
             m.jh = jh;
             push(t_mid_, m);
             it.kind = BATCH_ADJ_REF;
@@ -349,13 +361,14 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
             it.c = P.yh_.as<double>();
             it.d = ya;
             it.row = P.partial_.as<double>() + (size_t)(i - 1) * nsb;
-            it.jb = j.have_carry ? jy[j.cur_c] : nullptr;
+            it.jb = j.have_jcarry ? jy[j.cur_c] : nullptr;
             it.jh = jh;
             it.ja = jy[nxt];
             push(t_adj_, it);
             std::swap(j.z, j.z2);
             j.cur_c = nxt;
-            j.have_carry = true;
+            j.have_fcarry = fa == nullptr;
+            j.have_jcarry = true;
             break;
         }
         case Action::EXADJ: {

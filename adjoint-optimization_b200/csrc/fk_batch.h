@@ -38,7 +38,7 @@ struct Job {
     double* yT = nullptr;
     double *z = nullptr, *z2 = nullptr;
     int cur_c = 0;
-    bool have_carry = false;
+    bool have_fcarry = false, have_jcarry = false;  // f(y) / J(y) carried from the previous backward step
     bool finishing = false, done = false;
     fkadj_status status = FKADJ_OK;
     double* h_out = nullptr;  // pinned: [0] sum for L0, [1..rows] reductions

@@ -282,6 +282,7 @@ int64_t Problem::estimate_bytes(int nrows, int ncols, int nt, int n_num, int64_t
     } else {
         const int64_t c = std::max(2, (int)std::ceil(std::sqrt((double)nt)));
         b += ((nt + c - 1) / c + 1 + c - 1) * state;
+        if (grad_mode == FKADJ_GRAD_REF) b += (c - 1) * state;  // k1 kept by the segment recompute
     }
     return b;
 }

@@ -624,31 +624,35 @@ __device__ __forceinline__ int find_item(const BatchTick& t, int tile) {
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchTick t) {
+    pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
         const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
-        fwd_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, I.gh, it.E0, it.E1, it.E2, it.stages, tbx, tby, TY);
+        fwd_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, I.gh, it.E0, it.E1, it.E2, it.stages, tbx, tby, TY,
+                                  it.k1);
     }
 }
 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_batch_mid(const BatchInstance* __restrict__ inst, const BatchTick t, HermiteW hw) {
+    pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
         const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
         adj_mid_tile<TX, TY, NT>(I.P, I.g, it.a, it.b, I.gh, it.out, it.E0, it.E1, it.E2, hw, it.fin, it.fout,
-                                 it.jh, tbx, tby, TY);
+                                 it.jh, tbx, tby, TY, it.fa);
     }
 }
 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_batch_adj(const BatchInstance* __restrict__ inst, const BatchTick t) {
+    pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
         const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
         const BatchInstance& I = inst[it.inst];
@@ -959,7 +963,8 @@ cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchT
     DISPATCH(tile, {
         const size_t sm = stencil_smem<TX, TY>(NT);
         const int grid = persistent_grid(k_batch_fwd<TX, TY, NT>, NT, sm, t.tiles);
-        k_batch_fwd<TX, TY, NT><<<grid, NT, sm, st>>>(d_inst, t);
+        const cudaError_t e = launch_pdl(k_batch_fwd<TX, TY, NT>, dim3(grid), NT, sm, st, d_inst, t);
+        if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
 }
@@ -970,7 +975,8 @@ cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchT
     DISPATCH(tile, {
         const size_t sm = mid_smem<TX, TY>();
         const int grid = persistent_grid(k_batch_mid<TX, TY, NT>, NT, sm, t.tiles);
-        k_batch_mid<TX, TY, NT><<<grid, NT, sm, st>>>(d_inst, t, hw);
+        const cudaError_t e = launch_pdl(k_batch_mid<TX, TY, NT>, dim3(grid), NT, sm, st, d_inst, t, hw);
+        if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
 }
@@ -980,7 +986,8 @@ cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchT
     DISPATCH(tile, {
         const size_t sm = exact_smem<TX, TY>();
         const int grid = persistent_grid(k_batch_adj<TX, TY, NT>, NT, sm, t.tiles);
-        k_batch_adj<TX, TY, NT><<<grid, NT, sm, st>>>(d_inst, t);
+        const cudaError_t e = launch_pdl(k_batch_adj<TX, TY, NT>, dim3(grid), NT, sm, st, d_inst, t);
+        if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
 }

@@ -62,6 +62,8 @@ struct BatchItem {
     double E0, E1, E2;
     const double* fin;
     double *fout, *jh;
+    const double* fa;  // midpoint: kept f(ya) (null = evaluate)
+    double* k1;        // forward: where k1 = f(y) is kept (null = not kept)
     const double* jb;
     double* ja;
     double *row, *row2, *row3;
