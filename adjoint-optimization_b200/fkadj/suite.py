@@ -58,7 +58,7 @@ def cmd_ckpt(a):
 
 
 def _batch_insts(a):
-    if a.side > 0:  # `count` instances of one size, each with its own seeded geometry and pulse
+    if getattr(a, "side", 0) > 0:  # `count` instances of one size, each with its own seeded geometry and pulse
         return [W.make_instance(a.side, a.nt, seed=100 + k, n_obstacles=8, intervals=20) for k in range(a.count)]
     return W.batch_instances(count=a.count, seed=a.seed, max_side=a.max_side, nt_scale=a.nt_scale)
 
@@ -86,7 +86,7 @@ def cmd_batch(a):
         bt = time.perf_counter() - t0
         st = b.stats
     print(json.dumps({"suite": "batch", "count": a.count, "max_side": a.max_side, "nt_scale": a.nt_scale,
-                      "uniform": a.side > 0,
+                      "uniform": getattr(a, "side", 0) > 0,
                       "sides": sorted({i.nrows for i in insts}), "nt_range": [min(i.nt for i in insts),
                                                                               max(i.nt for i in insts)],
                       "sequential_s": seq, "batched_s": bt, "speedup": seq / bt,
