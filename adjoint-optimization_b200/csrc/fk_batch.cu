@@ -34,8 +34,14 @@ BatchEngine::~BatchEngine() {
         if (j->ev) cudaEventDestroy(j->ev);
         if (j->h_out) cudaFreeHost(j->h_out);
     }
+    for (auto& f : pinned_free_) cudaFreeHost(f.second);
+    pinned_free_.clear();
     jobs_.clear();
-    probs_.clear();
+    probs_.clear();  // their buffers go back to the pool in stream order
+    if (pool_) {
+        if (st_) cudaStreamSynchronize(st_);
+        cudaMemPoolDestroy(pool_);
+    }
     cudaFreeHost(t_fwd_);
     cudaFreeHost(t_mid_);
     cudaFreeHost(t_adj_);
@@ -56,6 +62,19 @@ fkadj_status BatchEngine::init(const fkadj_options* opt) {
     tiles_[0] = tiles_[1] = tiles_[2] = t;
     tuned_ = opt_.tile > 0 && opt_.tile <= tile_count();
     hw_ = hermite_weights();
+    {
+        // the problems' device memory: a pool of this engine, allocated and
+        // freed in stream order, kept reserved between requests
+        int dev = 0;
+        BCK(cudaGetDevice(&dev), "cudaGetDevice");
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        BCK(cudaMemPoolCreate(&pool_, &props), "memory pool");
+        uint64_t keep = UINT64_MAX;
+        BCK(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
+    }
     BCK(cudaMallocHost(&t_fwd_, sizeof(BatchTick)), "pinned tick");
     BCK(cudaMallocHost(&t_mid_, sizeof(BatchTick)), "pinned tick");
     BCK(cudaMallocHost(&t_adj_, sizeof(BatchTick)), "pinned tick");
@@ -73,6 +92,7 @@ fkadj_status BatchEngine::add_problem(const fkadj_params& p, double dt, int nt, 
     o.ckpt_budget_bytes = ckpt_budget;
     o.tile = tiles_[0] + 1;  // fixed preset: no per-problem autotune inside a batch
     auto pb = std::make_unique<Problem>();
+    pb->use_pool(pool_);
     const bool need_obj = gamma && S_colptr;
     fkadj_status s = pb->init(p, dt, nt, ai, nrows, ncols, n_num, gh_num, gamma, S_ncol, S_colptr, S_rowidx,
                               S_val, alpha, &o, need_obj);
@@ -111,8 +131,7 @@ fkadj_status BatchEngine::remove_problem(int id) {
             set_error("problem has a running job");
             return FKADJ_ERR_BUSY;
         }
-    BCK(cudaStreamSynchronize(st_), "synchronize");
-    probs_[id].reset();
+    probs_[id].reset();  // stream-ordered release: no synchronisation
     return FKADJ_OK;
 }
 
@@ -217,7 +236,11 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
         j->cur = P.state_buf(0);
     }
     if ((s = build_plan(*j))) return s;
-    BCK(cudaMallocHost(&j->h_out, sizeof(double) * (size_t)(j->rows + 1)), "pinned results");
+    j->h_out = take_pinned((size_t)j->rows + 1, &j->h_cap);
+    if (!j->h_out) {
+        set_error("pinned results: out of host memory");
+        return FKADJ_ERR_NOMEM;
+    }
     BCK(cudaEventCreateWithFlags(&j->ev, cudaEventDisableTiming), "event");
     j->t_start = host_seconds();
     *job_id = j->id;
@@ -544,9 +567,34 @@ fkadj_status BatchEngine::release_job(int id) {
         return FKADJ_ERR_BUSY;
     }
     if (j.ev) cudaEventDestroy(j.ev);
-    if (j.h_out) cudaFreeHost(j.h_out);
+    if (j.h_out) give_pinned(j.h_out, j.h_cap);
+    j.h_out = nullptr;
     jobs_[id].reset();
     return FKADJ_OK;
+}
+
+double* BatchEngine::take_pinned(size_t n, size_t* cap) {
+    // smallest free buffer that holds n doubles
+    int best = -1;
+    for (int k = 0; k < (int)pinned_free_.size(); ++k)
+        if (pinned_free_[k].first >= n && (best < 0 || pinned_free_[k].first < pinned_free_[best].first)) best = k;
+    if (best >= 0) {
+        double* p = pinned_free_[best].second;
+        *cap = pinned_free_[best].first;
+        pinned_free_.erase(pinned_free_.begin() + best);
+        return p;
+    }
+    double* p = nullptr;
+    if (cudaMallocHost(&p, n * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    *cap = n;
+    return p;
+}
+
+void BatchEngine::give_pinned(double* p, size_t cap) {
+    if (p) pinned_free_.push_back({cap, p});
 }
 
 }  // namespace fkadj

@@ -42,6 +42,7 @@ struct Job {
     bool finishing = false, done = false;
     fkadj_status status = FKADJ_OK;
     double* h_out = nullptr;  // pinned: [0] sum for L0, [1..rows] reductions
+    size_t h_cap = 0;         // doubles in h_out (a buffer of the engine's pool)
     int rows = 0;
     cudaEvent_t ev = nullptr;
     std::vector<double> Et;
@@ -92,6 +93,7 @@ private:
 
     cudaStream_t st_ = nullptr;
     bool own_stream_ = false;
+    cudaMemPool_t pool_ = nullptr;  // device memory of the engine's problems
     int tiles_[3] = {0, 0, 0};  // fwd, mid, adj presets
     bool tuned_ = false;        // presets fixed (options.tile > 0) or autotuned
     HermiteW hw_{};
@@ -106,6 +108,11 @@ private:
     BatchTick* t_adj_ = nullptr;
     int64_t launches_ = 0, ticks_ = 0;
     fkadj_options opt_{};
+    // Pinned result buffers, reused across jobs: cudaFreeHost synchronises the
+    // device, which would stall every running job each time one finishes.
+    std::vector<std::pair<size_t, double*>> pinned_free_;
+    double* take_pinned(size_t n, size_t* cap);
+    void give_pinned(double* p, size_t cap);
 };
 
 double host_seconds();

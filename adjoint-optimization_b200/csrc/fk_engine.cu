@@ -172,6 +172,12 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
         own_stream_ = true;
     }
     for (auto& e : ev_) CK(cudaEventCreate(&e), "cudaEventCreate");
+    if (pool_) {
+        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &work_,
+                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
+                         &fcache_, &Ed_};
+        for (DevBuf* b : all) b->st = st_, b->pool = pool_;
+    }
     {
         // stream capture needs a real stream; FKADJ_NO_GRAPHS=1 keeps plain launches
         const char* ng = getenv("FKADJ_NO_GRAPHS");
@@ -220,9 +226,10 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     CK(gh_.alloc(pl * sizeof(double)), "alloc gh");
     CK(wc_.alloc(pl), "alloc weights");
     CK(pos_.alloc((size_t)n_num * sizeof(long long)), "alloc positions");
-    CK(cudaMemcpy(gh_.p, gh.data(), pl * sizeof(double), cudaMemcpyHostToDevice), "upload gh");
-    CK(cudaMemcpy(wc_.p, wc.data(), pl, cudaMemcpyHostToDevice), "upload weights");
-    CK(cudaMemcpy(pos_.p, pos.data(), (size_t)n_num * sizeof(long long), cudaMemcpyHostToDevice),
+    // stream-ordered copies (from pageable memory they return once the data is staged)
+    CK(cudaMemcpyAsync(gh_.p, gh.data(), pl * sizeof(double), cudaMemcpyHostToDevice, st_), "upload gh");
+    CK(cudaMemcpyAsync(wc_.p, wc.data(), pl, cudaMemcpyHostToDevice, st_), "upload weights");
+    CK(cudaMemcpyAsync(pos_.p, pos.data(), (size_t)n_num * sizeof(long long), cudaMemcpyHostToDevice, st_),
        "upload positions");
 
     if (need_objective) {
@@ -250,10 +257,11 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
         CK(Srow_.alloc((n_num + 1) * sizeof(long long)), "alloc S");
         CK(Scol_.alloc(std::max<int64_t>(nnz, 1) * sizeof(int)), "alloc S");
         CK(Sval_.alloc(std::max<int64_t>(nnz, 1) * sizeof(double)), "alloc S");
-        CK(cudaMemcpy(Srow_.p, rp.data(), (n_num + 1) * sizeof(long long), cudaMemcpyHostToDevice), "upload S");
+        CK(cudaMemcpyAsync(Srow_.p, rp.data(), (n_num + 1) * sizeof(long long), cudaMemcpyHostToDevice, st_),
+           "upload S");
         if (nnz) {
-            CK(cudaMemcpy(Scol_.p, ci.data(), nnz * sizeof(int), cudaMemcpyHostToDevice), "upload S");
-            CK(cudaMemcpy(Sval_.p, cv.data(), nnz * sizeof(double), cudaMemcpyHostToDevice), "upload S");
+            CK(cudaMemcpyAsync(Scol_.p, ci.data(), nnz * sizeof(int), cudaMemcpyHostToDevice, st_), "upload S");
+            CK(cudaMemcpyAsync(Sval_.p, cv.data(), nnz * sizeof(double), cudaMemcpyHostToDevice, st_), "upload S");
         }
         have_obj_ = true;
     }
@@ -262,7 +270,7 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     CK(opart_.alloc((size_t)objective_blocks(n_num) * sizeof(double)), "alloc partials");
     CK(osum_.alloc(sizeof(double)), "alloc sum");
     CK(work_.alloc(3 * state_bytes()), "alloc states");
-    CK(cudaMemset(work_.p, 0xff, work_.bytes), "init states");
+    CK(cudaMemsetAsync(work_.p, 0xff, work_.bytes, st_), "init states");
     spline_ = new NakSpline(nt + 1, dt);
     return FKADJ_OK;
 }
@@ -626,12 +634,6 @@ fkadj_status Problem::ensure_adjoint_work(bool all_rows) {
     if (zgh_.bytes < prow * sizeof(double)) {
         CK(zgh_.alloc(prow * sizeof(double)), "alloc zgh");
         ++buf_gen_;
-    }
-    if (hres_n_ < prow + 1) {
-        if (hres_) cudaFreeHost(hres_);
-        hres_ = nullptr;
-        CK(cudaMallocHost(&hres_, (prow + 1) * sizeof(double)), "alloc pinned results");
-        hres_n_ = prow + 1;
     }
     return FKADJ_OK;
 }
@@ -1030,6 +1032,16 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     if ((s = plan_trajectory(tp))) return s;
     if ((s = ensure_traj(tp))) return s;
     if ((s = ensure_adjoint_work())) return s;
+    // pinned results of the standalone gradient (the batch engine has its own:
+    // freeing pinned memory synchronises the device, which a batch must not do
+    // per job)
+    const size_t prow = (size_t)(3 * nt_ + 1);
+    if (hres_n_ < prow + 1) {
+        if (hres_) cudaFreeHost(hres_);
+        hres_ = nullptr;
+        CK(cudaMallocHost(&hres_, (prow + 1) * sizeof(double)), "alloc pinned results");
+        hres_n_ = prow + 1;
+    }
     const int nt = nt_;
     CK(cudaEventRecord(ev_[0], st_), "event");
     // ---- forward sweep, storing states (cu-G:1689-1724 without the D2H copies)

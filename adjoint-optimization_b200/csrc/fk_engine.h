@@ -19,23 +19,31 @@ namespace fkadj {
 
 void set_error(const std::string& msg);
 
-// One device allocation released on destruction.
+// One device allocation released on destruction.  With a memory pool set
+// (problems owned by a batch engine) allocation and release are stream-ordered
+// on `st`: releasing needs no device synchronisation, so a finished request can
+// free its memory while the others keep running.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pool) cudaFreeAsync(p, st);
+            else cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
     }
     cudaError_t alloc(size_t b) {
         release();
         if (b == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&p, b);
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, b, pool, st) : cudaMalloc(&p, b);
         if (e == cudaSuccess) bytes = b;
         else p = nullptr;
         return e;
@@ -95,6 +103,8 @@ public:
     cudaStream_t stream() const { return st_; }
     // tile preset per kernel kind; chosen by autotune() unless fixed by options
     enum TileKind { T_FWD = 0, T_MID = 1, T_ADJ = 2, T_EXACT = 3 };
+    // Stream-ordered device memory from `pool` (call before init).
+    void use_pool(cudaMemPool_t pool) { pool_ = pool; }
     int tile(int kind) const { return tk_[kind]; }
     void set_tile(int kind, int t) { tk_[kind] = t; }
     // rows per tile in use for a kernel kind (the preset's height, or fewer
@@ -174,6 +184,7 @@ private:
     int ty_[4] = {0, 0, 0, 0};  // rows per tile per kind (0 = the preset's height)
     bool autotune_ = true, tuned_ = false, tuned_fwd_ = false;
     bool own_stream_ = false, have_obj_ = false;
+    cudaMemPool_t pool_ = nullptr;
     int grad_mode_ = FKADJ_GRAD_REF, ckpt_policy_ = FKADJ_CKPT_AUTO;
     int64_t ckpt_budget_ = 0;
     cudaStream_t st_ = nullptr;
