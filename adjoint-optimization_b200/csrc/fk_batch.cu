@@ -58,7 +58,7 @@ fkadj_status BatchEngine::init(const fkadj_options* opt) {
         BCK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
         own_stream_ = true;
     }
-    const int t = (opt_.tile > 0 && opt_.tile <= tile_count()) ? opt_.tile - 1 : 0;
+    const int t = batch_preset((opt_.tile > 0 && opt_.tile <= tile_count()) ? opt_.tile - 1 : 0);
     tiles_[0] = tiles_[1] = tiles_[2] = t;
     tuned_ = opt_.tile > 0 && opt_.tile <= tile_count();
     hw_ = hermite_weights();
@@ -479,9 +479,10 @@ fkadj_status BatchEngine::tick(int* active) {
             P.autotune_ = true;
             if ((s = P.autotune())) return s;
             P.autotune_ = keep;
-            tiles_[0] = P.tk_[Problem::T_FWD];
-            tiles_[1] = P.tk_[Problem::T_MID];
-            tiles_[2] = P.grad_mode_ == FKADJ_GRAD_EXACT ? P.tk_[Problem::T_EXACT] : P.tk_[Problem::T_ADJ];
+            tiles_[0] = batch_preset(P.tk_[Problem::T_FWD]);
+            tiles_[1] = batch_preset(P.tk_[Problem::T_MID]);
+            tiles_[2] = batch_preset(P.grad_mode_ == FKADJ_GRAD_EXACT ? P.tk_[Problem::T_EXACT]
+                                                                       : P.tk_[Problem::T_ADJ]);
             tuned_ = true;
         }
     }

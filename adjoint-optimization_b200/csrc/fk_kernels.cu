@@ -662,6 +662,10 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
 
 // ---------------------------------------------------------------- batched
 //
+// The batched kernels hold more live state than the single-instance ones (the
+// work-queue item, the tile loop) and take up to 128 registers; their launch
+// bounds ask for one resident CTA only, so they never spill, and the engine runs
+// them with presets of at most 512 threads (batch_preset).
 // One launch per kernel kind and tick runs the tiles of every instance that
 // has that kind of work this tick.  The tick's work queue is passed by value
 // (no per-tick copies, so a tick is a plain launch that a CUDA graph can
@@ -679,7 +683,7 @@ __device__ __forceinline__ int find_item(const BatchTick& t, int tile) {
 }
 
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+__global__ void __launch_bounds__(NT, 1)
     k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchTick t) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
@@ -693,7 +697,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
 }
 
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+__global__ void __launch_bounds__(NT, 1)
     k_batch_mid(const BatchInstance* __restrict__ inst, const BatchTick t, HermiteW hw) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
@@ -707,7 +711,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
 }
 
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
+__global__ void __launch_bounds__(NT, 1)
     k_batch_adj(const BatchInstance* __restrict__ inst, const BatchTick t) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
@@ -874,6 +878,14 @@ static int persistent_grid(K kernel, int nt, size_t smem, int tiles) {
     X(7, 32, 32, 384)
 
 int tile_count() { return 8; }
+
+int batch_preset(int t) {
+    // 64x32/768 -> 64x32/512, 32x32/384 -> 32x32/512: more threads per CTA would
+    // cap the batched kernels below the registers they need
+    if (t == 6) return 2;
+    if (t == 7) return 1;
+    return t;
+}
 
 TileShape tile_shape(int t) {
     switch (t) {

@@ -84,6 +84,8 @@ cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchT
 cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st);
 
 int tile_count();
+// The preset the batched kernels run for an autotuned single-instance preset.
+int batch_preset(int tile);
 TileShape tile_shape(int tile);
 int tiles_of(int tile, const DevGrid& g);
 cudaError_t kernels_init();
