@@ -45,6 +45,9 @@ BatchEngine::~BatchEngine() {
     cudaFreeHost(t_fwd_);
     cudaFreeHost(t_mid_);
     cudaFreeHost(t_adj_);
+    for (auto& e : qev_)
+        if (e) cudaEventDestroy(e);
+    if (qring_) cudaFreeHost(qring_);
     if (own_stream_ && st_) cudaStreamDestroy(st_);
 }
 
@@ -75,6 +78,8 @@ fkadj_status BatchEngine::init(const fkadj_options* opt) {
         uint64_t keep = UINT64_MAX;
         BCK(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
     }
+    BCK(cudaMallocHost(&qring_, sizeof(BatchItem) * (size_t)kQueueRing * 3 * kBatchMaxItems), "queue ring");
+    BCK(qdev_.alloc(sizeof(BatchItem) * 3 * kBatchMaxItems), "device queue");
     BCK(cudaMallocHost(&t_fwd_, sizeof(BatchTick)), "pinned tick");
     BCK(cudaMallocHost(&t_mid_, sizeof(BatchTick)), "pinned tick");
     BCK(cudaMallocHost(&t_adj_, sizeof(BatchTick)), "pinned tick");
@@ -512,9 +517,29 @@ fkadj_status BatchEngine::tick(int* active) {
     }
     active_.swap(still);
     const BatchInstance* inst = inst_dev_.as<BatchInstance>();
-    BCK(launch_batch_fwd(tiles_[0], inst, *t_fwd_, st_), "batched forward");
-    BCK(launch_batch_mid(tiles_[1], inst, *t_mid_, hw_, st_), "batched midpoint");
-    BCK(launch_batch_adj(tiles_[2], inst, *t_adj_, st_), "batched adjoint");
+    // the three queues, packed into the next pinned ring slot and copied to the
+    // device queue in one stream-ordered copy (the previous tick's kernels are
+    // done with it by then); a slot is reused kQueueRing ticks later, after its
+    // copy's event
+    const int nf = t_fwd_->n, nm = t_mid_->n, na = t_adj_->n;
+    if (nf + nm + na > 0) {
+        const int k = (int)(qcount_++ % kQueueRing);
+        if (qev_[k]) BCK(cudaEventSynchronize(qev_[k]), "queue slot");
+        else BCK(cudaEventCreateWithFlags(&qev_[k], cudaEventDisableTiming), "queue event");
+        BatchItem* slot = qring_ + (size_t)k * 3 * kBatchMaxItems;
+        std::copy(t_fwd_->item, t_fwd_->item + nf, slot);
+        std::copy(t_mid_->item, t_mid_->item + nm, slot + nf);
+        std::copy(t_adj_->item, t_adj_->item + na, slot + nf + nm);
+        BatchItem* dq = qdev_.as<BatchItem>();
+        BCK(cudaMemcpyAsync(dq, slot, sizeof(BatchItem) * (size_t)(nf + nm + na), cudaMemcpyHostToDevice, st_),
+            "upload queue");
+        BCK(cudaEventRecord(qev_[k], st_), "queue event");
+        BCK(launch_batch_fwd(tiles_[0], inst, BatchQueue{dq, nf, t_fwd_->tiles}, st_), "batched forward");
+        BCK(launch_batch_mid(tiles_[1], inst, BatchQueue{dq + nf, nm, t_mid_->tiles}, hw_, st_),
+            "batched midpoint");
+        BCK(launch_batch_adj(tiles_[2], inst, BatchQueue{dq + nf + nm, na, t_adj_->tiles}, st_),
+            "batched adjoint");
+    }
     launches_ += (t_fwd_->n > 0) + (t_mid_->n > 0) + (t_adj_->n > 0);
     ++ticks_;
     if (active) *active = (int)active_.size();

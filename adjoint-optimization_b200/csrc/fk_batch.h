@@ -103,6 +103,11 @@ private:
     bool inst_dirty_ = true;
     std::vector<std::unique_ptr<Job>> jobs_;
     std::vector<int> active_;  // job ids in tick order
+    static constexpr int kQueueRing = 64;
+    BatchItem* qring_ = nullptr;        // pinned: kQueueRing slots of 3 x kBatchMaxItems items
+    cudaEvent_t qev_[kQueueRing] = {};  // a slot's copy has run
+    uint64_t qcount_ = 0;
+    DevBuf qdev_;                       // the device queue the kernels read
     BatchTick* t_fwd_ = nullptr;  // host staging of the three queues
     BatchTick* t_mid_ = nullptr;
     BatchTick* t_adj_ = nullptr;

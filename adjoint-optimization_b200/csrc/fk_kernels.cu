@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <utility>
+#include <vector>
 
 namespace fkadj {
 
@@ -667,16 +668,15 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
 // bounds ask for one resident CTA only, so they never spill, and the engine runs
 // them with presets of at most 512 threads (batch_preset).
 // One launch per kernel kind and tick runs the tiles of every instance that
-// has that kind of work this tick.  The tick's work queue is passed by value
-// (no per-tick copies, so a tick is a plain launch that a CUDA graph can
-// hold); a persistent grid of CTAs strides over the queue's tiles, each item
-// owning a contiguous range of tile indices.
-template <int TX, int TY, int NT>
-__device__ __forceinline__ int find_item(const BatchTick& t, int tile) {
-    int lo = 0, hi = t.n - 1;
+// has that kind of work this tick.  The tick's work queue is in device memory
+// (one small copy per tick; kernel parameters stay a few bytes); a persistent
+// grid of CTAs strides over the queue's tiles, each item owning a contiguous
+// range of tile indices.
+__device__ __forceinline__ int find_item(const BatchQueue& q, int tile) {
+    int lo = 0, hi = q.n - 1;
     while (lo < hi) {  // last item whose first tile is <= tile
         const int mid = (lo + hi + 1) >> 1;
-        if (t.item[mid].tile0 <= tile) lo = mid;
+        if (q.items[mid].tile0 <= tile) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -684,10 +684,10 @@ __device__ __forceinline__ int find_item(const BatchTick& t, int tile) {
 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 1)
-    k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchTick t) {
+    k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
-        const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
+        const BatchItem& it = t.items[find_item(t, tile)];
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
@@ -698,10 +698,10 @@ __global__ void __launch_bounds__(NT, 1)
 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 1)
-    k_batch_mid(const BatchInstance* __restrict__ inst, const BatchTick t, HermiteW hw) {
+    k_batch_mid(const BatchInstance* __restrict__ inst, const BatchQueue t, HermiteW hw) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
-        const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
+        const BatchItem& it = t.items[find_item(t, tile)];
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
@@ -712,10 +712,10 @@ __global__ void __launch_bounds__(NT, 1)
 
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 1)
-    k_batch_adj(const BatchInstance* __restrict__ inst, const BatchTick t) {
+    k_batch_adj(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
-        const BatchItem& it = t.item[find_item<TX, TY, NT>(t, tile)];
+        const BatchItem& it = t.items[find_item(t, tile)];
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
@@ -858,9 +858,16 @@ static int persistent_grid(K kernel, int nt, size_t smem, int tiles) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 1;
     }
+    // occupancy per kernel, computed once (a per-tick query costs host time)
+    static thread_local std::vector<std::pair<const void*, int>> occ;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
+    for (auto& o : occ)
+        if (o.first == (const void*)kernel) per_sm = o.second;
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        occ.push_back({(const void*)kernel, per_sm});
+    }
     const int g = sms * per_sm;
     return tiles < g ? tiles : g;
 }
@@ -1027,7 +1034,7 @@ cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st) {
+cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchQueue& t, cudaStream_t st) {
     if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
     DISPATCH(tile, {
         const size_t sm = stencil_smem<TX, TY>(NT);
@@ -1038,7 +1045,7 @@ cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchT
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchTick& t, const HermiteW& hw,
+cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchQueue& t, const HermiteW& hw,
                              cudaStream_t st) {
     if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
     DISPATCH(tile, {
@@ -1050,7 +1057,7 @@ cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchT
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st) {
+cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchQueue& t, cudaStream_t st) {
     if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
     DISPATCH(tile, {
         const size_t sm = exact_smem<TX, TY>();

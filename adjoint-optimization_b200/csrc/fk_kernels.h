@@ -71,17 +71,25 @@ struct BatchItem {
 
 constexpr int kBatchMaxItems = 128;
 
-// A tick's work queue for one kernel kind, passed to the launch by value.
+// A tick's work queue for one kernel kind, as the host builds it.
 struct BatchTick {
     int n;      // items
     int tiles;  // total tiles
     BatchItem item[kBatchMaxItems];
 };
 
-cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st);
-cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchTick& t, const HermiteW& hw,
+// A tick's work queue of one kernel kind as the kernels read it: n items in
+// device memory, `tiles` tiles in all.
+struct BatchQueue {
+    const BatchItem* items;
+    int n;
+    int tiles;
+};
+
+cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchQueue& q, cudaStream_t st);
+cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchQueue& q, const HermiteW& hw,
                              cudaStream_t st);
-cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchTick& t, cudaStream_t st);
+cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchQueue& q, cudaStream_t st);
 
 int tile_count();
 // The preset the batched kernels run for an autotuned single-instance preset.

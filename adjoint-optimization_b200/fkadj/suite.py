@@ -10,7 +10,8 @@
   python -m fkadj.suite serve  [--rates 10,50,200,500 --requests 48 ...]
       Poisson arrivals, half objective-only, half objective+gradient, sizes as
       above: served latency p50/p99 and throughput, against the same stream
-      solved one request at a time (FIFO, each request's standalone time)
+      solved one request at a time (FIFO): as plain solves of new instances
+      (set-up included) and as warm resident calls
 
   python -m fkadj.suite opt   [--n 2048 --nt 100000 --iters 1 --probes 4 --budget-gb 60]
       the optimisation loop at scale: Armijo descent on the interval
@@ -100,14 +101,18 @@ def cmd_serve(a):
     base = _batch_insts(argparse.Namespace(count=a.requests, seed=a.seed, max_side=a.max_side,
                                            nt_scale=a.nt_scale))
     grads = [bool(x) for x in rng.integers(0, 2, size=a.requests)]
-    # standalone service time of every request (for the sequential baseline)
-    service = []
+    # standalone service time of every request, two ways: a plain solve of a new
+    # instance (problem set-up, upload, autotune and the call: what one request
+    # costs without the server) and a warm resident call (set-up excluded)
+    service, service_warm = [], []
     for inst, g in zip(base, grads):
+        t0 = time.perf_counter()
         with api.Problem(inst, opts=api.options(ckpt_policy=_lib.CKPT_SQRT)) as pb:
             (pb.grad if g else pb.objective)(inst.Et, inst.y0)
+            service.append(time.perf_counter() - t0)
             t0 = time.perf_counter()
             (pb.grad if g else pb.objective)(inst.Et)
-            service.append(time.perf_counter() - t0)
+            service_warm.append(time.perf_counter() - t0)
     for rate in a.rates:
         gaps = rng.exponential(1.0 / rate, size=a.requests)
         arrive = np.cumsum(gaps) - gaps[0]
@@ -126,17 +131,22 @@ def cmd_serve(a):
             makespan = time.perf_counter() - t0
             peak = srv.stats["peak_running"]
         # sequential FIFO plain solves with the same arrivals
-        fin, seq_lat = 0.0, []
-        for k in range(a.requests):
-            start = max(arrive[k], fin)
-            fin = start + service[k]
-            seq_lat.append(fin - arrive[k])
+        def fifo(svc):
+            fin, out = 0.0, []
+            for k in range(a.requests):
+                fin = max(arrive[k], fin) + svc[k]
+                out.append(fin - arrive[k])
+            return fin, out
+        fin, seq_lat = fifo(service)
+        fin_w, seq_w = fifo(service_warm)
         print(json.dumps({"suite": "serve", "rate_req_s": rate, "requests": a.requests,
                           "max_side": a.max_side, "nt_scale": a.nt_scale,
                           "served_p50_s": _pct(lat, 50), "served_p99_s": _pct(lat, 99),
                           "served_throughput_req_s": a.requests / makespan,
                           "sequential_p50_s": _pct(seq_lat, 50), "sequential_p99_s": _pct(seq_lat, 99),
                           "sequential_throughput_req_s": a.requests / fin,
+                          "sequential_warm_p50_s": _pct(seq_w, 50), "sequential_warm_p99_s": _pct(seq_w, 99),
+                          "sequential_warm_throughput_req_s": a.requests / fin_w,
                           "peak_running": peak}), flush=True)
 
 
