@@ -43,6 +43,13 @@ __device__ __forceinline__ void pdl_enter() {
 #ifndef FKADJ_STAGE_UNROLL
 #define FKADJ_STAGE_UNROLL 1
 #endif
+// Resident CTAs per SM the batched kernels' register allocation targets: 1
+// (no spills, up to 128+ registers) or the single-instance kernels' choice.
+#ifndef FKADJ_BATCH_ONE_CTA
+#define FKADJ_BATCH_ONE_CTA 1
+#endif
+#define FKADJ_BATCH_MINB(tx, ty, nt) (FKADJ_BATCH_ONE_CTA ? 1 : min_blocks(tx, ty, nt))
+
 // Software-pipelined global loads in the cached-Jacobian adjoint stages.
 #ifndef FKADJ_ADJ_PREFETCH
 #define FKADJ_ADJ_PREFETCH 0
@@ -683,7 +690,7 @@ __device__ __forceinline__ int find_item(const BatchQueue& q, int tile) {
 }
 
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
@@ -697,7 +704,7 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_mid(const BatchInstance* __restrict__ inst, const BatchQueue t, HermiteW hw) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
@@ -711,7 +718,7 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_adj(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
     for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
