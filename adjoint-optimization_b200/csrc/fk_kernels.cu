@@ -43,10 +43,13 @@ __device__ __forceinline__ void pdl_enter() {
 #ifndef FKADJ_STAGE_UNROLL
 #define FKADJ_STAGE_UNROLL 1
 #endif
-// Resident CTAs per SM the batched kernels' register allocation targets: 1
-// (no spills, up to 128+ registers) or the single-instance kernels' choice.
+// Resident CTAs per SM the batched kernels' register allocation targets: the
+// single-instance kernels' choice (default; the 256-thread presets then spill a
+// little but keep two or three CTAs per SM, which measured faster: 32 x 128^2
+// batched 0.58 s against 0.71 s, 16 x 256^2 0.48 s against 0.72 s), or 1 (no
+// spills).
 #ifndef FKADJ_BATCH_ONE_CTA
-#define FKADJ_BATCH_ONE_CTA 1
+#define FKADJ_BATCH_ONE_CTA 0
 #endif
 #define FKADJ_BATCH_MINB(tx, ty, nt) (FKADJ_BATCH_ONE_CTA ? 1 : min_blocks(tx, ty, nt))
 
@@ -671,9 +674,9 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
 // ---------------------------------------------------------------- batched
 //
 // The batched kernels hold more live state than the single-instance ones (the
-// work-queue item, the tile loop) and take up to 128 registers; their launch
-// bounds ask for one resident CTA only, so they never spill, and the engine runs
-// them with presets of at most 512 threads (batch_preset).
+// work-queue item, the tile loop) and want up to 128 registers; the engine runs
+// them with presets of at most 512 threads (batch_preset), where the 768- and
+// 384-thread presets would cap them at 80 registers and spill heavily.
 // One launch per kernel kind and tick runs the tiles of every instance that
 // has that kind of work this tick.  The tick's work queue is in device memory
 // (one small copy per tick; kernel parameters stay a few bytes); a persistent
