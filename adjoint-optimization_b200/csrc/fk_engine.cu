@@ -11,8 +11,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace fkadj {
@@ -638,7 +640,47 @@ fkadj_status Problem::ensure_adjoint_work(bool all_rows) {
     return FKADJ_OK;
 }
 
+// Autotuned tiles by (device, grid shape, gradient mode): problems created
+// later with the same key take them without trial launches (the drop-in
+// entry points create a problem per call).  Results do not depend on tiles.
+namespace {
+struct TuneKey {
+    int dev, nrows, ncols, mode;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(dev, nrows, ncols, mode) < std::tie(o.dev, o.nrows, o.ncols, o.mode);
+    }
+};
+struct TuneVal {
+    int tk[4], ty[4];
+    bool adjoint;  // the adjoint kinds were tuned too
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+}  // namespace
+
 fkadj_status Problem::autotune() {
+    const bool want_adjoint = zbuf_.p != nullptr;
+    const TuneKey key{device_, g_.nrows, g_.ncols, grad_mode_};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end() && (it->second.adjoint || !want_adjoint)) {
+            for (int k = 0; k < 4; ++k) tk_[k] = it->second.tk[k], ty_[k] = it->second.ty[k];
+            return FKADJ_OK;
+        }
+    }
+    const fkadj_status ts = autotune_trials();
+    if (ts == FKADJ_OK) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        TuneVal v;
+        for (int k = 0; k < 4; ++k) v.tk[k] = tk_[k], v.ty[k] = ty_[k];
+        v.adjoint = want_adjoint;
+        g_tune[key] = v;
+    }
+    return ts;
+}
+
+fkadj_status Problem::autotune_trials() {
     const double* y = y0res_.as<double>();
     double* out = state_buf(1);
     cudaEvent_t a = nullptr, b = nullptr;

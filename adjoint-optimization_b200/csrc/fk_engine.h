@@ -114,6 +114,7 @@ public:
     // state (a few launches each) and keeps the fastest per kind.  Results do
     // not depend on the choice (fixed-order reductions).
     fkadj_status autotune();
+    fkadj_status autotune_trials();
 
     // Lower-level pieces (used by the batch / serving layers and the tests).
     // upload_state with y_ini == nullptr re-uses the initial state of the
