@@ -892,14 +892,15 @@ static int persistent_grid(K kernel, int nt, size_t smem, int tiles) {
     X(4, 16, 16, 256)      \
     X(5, 64, 16, 512)      \
     X(6, 64, 32, 768)      \
-    X(7, 32, 32, 384)
+    X(7, 32, 32, 384)      \
+    X(8, 64, 32, 640)
 
-int tile_count() { return 8; }
+int tile_count() { return 9; }
 
 int batch_preset(int t) {
-    // 64x32/768 -> 64x32/512, 32x32/384 -> 32x32/512: more threads per CTA would
+    // 64x32/768 and /640 -> 64x32/512, 32x32/384 -> 32x32/512: more threads per CTA would
     // cap the batched kernels below the registers they need
-    if (t == 6) return 2;
+    if (t == 6 || t == 8) return 2;
     if (t == 7) return 1;
     return t;
 }
@@ -964,6 +965,7 @@ static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, int threads, 
         case 5: { constexpr int TX = 64, TY = 16, NT = 512; __VA_ARGS__; } break; \
         case 6: { constexpr int TX = 64, TY = 32, NT = 768; __VA_ARGS__; } break; \
         case 7: { constexpr int TX = 32, TY = 32, NT = 384; __VA_ARGS__; } break; \
+        case 8: { constexpr int TX = 64, TY = 32, NT = 640; __VA_ARGS__; } break; \
         default: { constexpr int TX = 32, TY = 32, NT = 256; __VA_ARGS__; } break; \
     }
 

@@ -40,7 +40,7 @@ def test_forward_matches_oracle(shape):
     assert "h = 0.025" in pstr
 
 
-@pytest.mark.parametrize("tile", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("tile", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_forward_state_is_independent_of_tile_shape(tile):
     """options.tile k >= 1 fixes preset k-1 for every kernel; 0 autotunes."""
     inst = _inst(96, 40, seed=3, ncols=72)
@@ -58,7 +58,7 @@ def test_gradient_bits_are_independent_of_tile_and_autotune(mode):
     autotuned choice give bit-identical gradients."""
     inst = _inst(80, 60, seed=13, ncols=112, objective="gradient")
     outs = []
-    for tile in (0, 1, 2, 3, 4, 5, 6):
+    for tile in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9):
         outs.append(api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols,
                                    inst.nrows, inst.ghost, inst.gamma, inst.S, 0.1, params=inst.params,
                                    opts=api.options(tile=tile, grad_mode=mode)))
