@@ -37,7 +37,10 @@ def _f64(a):
 
 def compute_ns(nt: int, nstep: int) -> int:
     """Number of forward snapshots (fk_forward_Et_param_mex.cpp:7-25): the final
-    step is not stored when nt/nstep is an integer."""
+    step is not stored when nt/nstep is an integer.  nstep <= 0 asks for no
+    snapshots (the reference's rule divides by nstep)."""
+    if nstep <= 0:
+        return 0
     r = nt / nstep
     rn = round(r)
     if abs(r - rn) < 5e-16 * r:

@@ -101,3 +101,28 @@ def test_forward_driver_writes_the_snapshots_the_library_computes(tmp_path):
     _, ora = O.forward(inst.params, inst.dt, inst.Et, inst.nt, inst.nrows, inst.ncols, inst.y0_grid, inst.gh_grid)
     act = np.isfinite(yf)
     assert np.max(np.abs(yf[act] - ora[act])) <= 1e-10 * np.max(np.abs(ora[act]))
+
+
+def test_gradient_descent_driver_armijo_mode_decreases_the_cost(tmp_path):
+    """line_search = 'armijo' with the exact gradient: trial steps as one batch
+    of objective-only jobs; every accepted step lowers Lcost, so the recorded
+    Lcost_vec never increases."""
+    inst = W.make_instance(64, 300, seed=71, n_obstacles=5, intervals=12, objective="gradient", alpha=0.02)
+    ai = inst.active_index.astype(np.int32)
+    matio.savemat(str(tmp_path / "grid.mat"), {"active_index": ai, "ghost_lr": inst.ghost.astype(np.float64)})
+    matio.savemat(str(tmp_path / "S.mat"), {"S": inst.S})
+    matio.savemat(str(tmp_path / "ic.mat"), {"yf": _nan_grid(inst.y0, ai)})
+    matio.savemat(str(tmp_path / "seed.mat"), {"Et": inst.Et.reshape(1, -1)})
+    (tmp_path / "infile_grad").write_text(
+        f"alpha = 0.02;\nds = 1e-2;\nns = 4;\nfinal_time = {inst.dt * inst.nt!r};\ndt = {inst.dt!r};\n"
+        "gamma = [1, 0.2, 0.2];\nnmod = 4;\nEt_seed_file = 'seed.mat';\nicondfile = 'ic.mat';\n"
+        "grid_file = 'grid.mat';\nS_file = 'S.mat';\nmex_function = @fk_grad_Et_mex;\nin_path = './';\n"
+        f"out_path = './';\njobid = 'armijo';\ndx = {inst.dx!r};\ngrad_mode = 'exact';\n"
+        "line_search = 'armijo';\nprobes = 5;\n")
+    r = _run("fkadj_simple_grad_desc", tmp_path)
+    assert r.stdout.count("armijo:") == 4
+    outs = [f for f in os.listdir(tmp_path) if f.startswith("simple_grad_desc_step_") and f.endswith("_armijo_4.mat")]
+    assert len(outs) == 1, os.listdir(tmp_path)
+    L = sio.loadmat(str(tmp_path / outs[0]))["Lcost_vec"].ravel()
+    assert np.all(np.diff(L) <= 0), L
+    assert "accepted" in r.stdout

@@ -43,7 +43,8 @@ def test_graph_replay_is_bit_identical_to_plain_launches(mode, ckpt, budget):
             b = pp.grad(E, y0)
             assert np.array_equal(a["gradE"], b["gradE"]), k
             assert a["Lcost"] == b["Lcost"] and a["L0"] == b["L0"]
-            assert pg.last_launches == pp.last_launches
+            if k > 0:  # the first call of the first problem also runs the autotuner's trials
+                assert pg.last_launches == pp.last_launches
 
 
 def test_profiling_and_graph_runs_agree():
