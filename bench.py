@@ -371,7 +371,7 @@ def main():
     ap.add_argument("--ckpt", default="sqrt", choices=["sqrt", "full", "auto"])
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cpu-steps", type=int, default=24)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-full", action="store_true", help="skip the full-trajectory comparison")
     ap.add_argument("--full-steps", type=int, default=2)
