@@ -53,10 +53,6 @@ __device__ __forceinline__ void pdl_enter() {
 #endif
 #define FKADJ_BATCH_MINB(tx, ty, nt) (FKADJ_BATCH_ONE_CTA ? 1 : min_blocks(tx, ty, nt))
 
-// Software-pipelined global loads in the cached-Jacobian adjoint stages.
-#ifndef FKADJ_ADJ_PREFETCH
-#define FKADJ_ADJ_PREFETCH 0
-#endif
 constexpr int kStageUnroll = FKADJ_STAGE_UNROLL;
 
 // Resident CTAs per SM the register allocation targets: what shared memory
@@ -399,59 +395,6 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
     constexpr int IN = TX * TY;
-#if FKADJ_ADJ_PREFETCH
-    // Cached-Jacobian stages (never the last): the global operands of the
-    // thread's next cell are loaded before this cell is computed.
-    if (MODE != 2 && jload) {
-        struct Pre {
-            double a, b, e;
-            int code;
-            JacT J;
-        };
-        auto fetch = [&](int q, Pre& p) {
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
-            const long long o = off + (long long)r * g.ld + c;
-            p.a = __ldg(z0g + o);
-            p.b = __ldg(z0g + g.plane + o);
-            p.e = __ldg(z0g + 2 * g.plane + o);
-            p.code = __ldg(wc + o);
-            p.J = load_jac(jload, g.plane, o);
-        };
-        Pre cur;
-        if ((int)threadIdx.x < N) fetch(threadIdx.x, cur);
-        for (int q = threadIdx.x; q < N; q += NT) {
-            Pre nxt;
-            if (q + NT < N) fetch(q + NT, nxt);
-            const int r = HALO - E + q / W, c = HALO - E + q % W;
-            const int s = r * RW + c;
-            double ku, kv, kw;
-            if (isnan(src[s])) {
-                ku = kv = kw = src[s];
-            } else {
-                adj_at<RW, RN>(P, src, s, cur.code, cur.J, ku, kv, kw);
-            }
-            const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
-            const int d = (r - HALO) * TX + (c - HALO);
-            dst[s] = cur.a + cZ * ku;
-            dst[RN + s] = cur.b + cZ * kv;
-            dst[2 * RN + s] = cur.e + cZ * kw;
-            if (inner) {
-                if (MODE == 0) {
-                    D[d] = cD * ku;
-                    D[IN + d] = cD * kv;
-                    D[2 * IN + d] = cD * kw;
-                } else {
-                    D[d] = D[d] + cD * ku;
-                    D[IN + d] = D[IN + d] + cD * kv;
-                    D[2 * IN + d] = D[2 * IN + d] + cD * kw;
-                }
-            }
-            cur = nxt;
-        }
-        __syncthreads();
-        return;
-    }
-#endif
 #pragma unroll kStageUnroll
     for (int q = threadIdx.x; q < N; q += NT) {
         const int r = HALO - E + q / W, c = HALO - E + q % W;
