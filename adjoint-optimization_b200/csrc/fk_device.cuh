@@ -72,8 +72,11 @@ __device__ __forceinline__ void steps_pq(const DevModel& P, double u, Step& sp, 
 
 // Ionic currents (formula of cu-F:29-45): p, q and (1 + tanh)/2 of the slow
 // inward current are the three smoothed steps.
-__device__ __forceinline__ void fk_ion_from(const DevModel& P, double u, double v, double w, const Step& sp,
-                                            const Step& sq, const Step& ss, double& ud, double& vd, double& wd) {
+__device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, double w,
+                                       double& ud, double& vd, double& wd) {
+    Step sp, sq;
+    steps_pq(P, u, sp, sq);
+    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
     const double p = sp.s, q = sq.s;
     const double j_fi = -v * p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
     const double j_so = u * sp.c * P.r_tau_0 + p * P.r_tau_r;
@@ -84,14 +87,6 @@ __device__ __forceinline__ void fk_ion_from(const DevModel& P, double u, double 
     wd = (sp.c * (1.0 - w)) * P.r_tau_wm - (p * w) * P.r_tau_wp;
 }
 
-__device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, double w,
-                                       double& ud, double& vd, double& wd) {
-    Step sp, sq;
-    steps_pq(P, u, sp, sq);
-    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
-    fk_ion_from(P, u, v, w, sp, sq, ss, ud, vd, wd);
-}
-
 // The seven non-zero entries of the transposed Jacobian of fk_ion
 // (formula of cu-G:1160-1184): jt[0]=du'/du, jt[1]=dv'/du, jt[2]=dw'/du,
 // jt[3]=du'/dv, jt[4]=dv'/dv, jt[5]=du'/dw, jt[6]=dw'/dw.
@@ -100,8 +95,10 @@ struct JacT {
 };
 
 // 1 - tanh^2 = 4 s (1 - s) for the smoothed step s.
-__device__ __forceinline__ JacT fk_jacT_from(const DevModel& P, double u, double v, double w, const Step& sp,
-                                             const Step& sq, const Step& ss) {
+__device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, double w) {
+    Step sp, sq;
+    steps_pq(P, u, sp, sq);
+    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
     const double p = sp.s, q = sq.s;
     const double dp = 4.0 * sp.s * sp.c;
     const double dq = 4.0 * sq.s * sq.c;
@@ -123,13 +120,6 @@ __device__ __forceinline__ JacT fk_jacT_from(const DevModel& P, double u, double
     return J;
 }
 
-__device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, double w) {
-    Step sp, sq;
-    steps_pq(P, u, sp, sq);
-    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
-    return fk_jacT_from(P, u, v, w, sp, sq, ss);
-}
-
 // u as the exponentials see it.  Without the hole branch, holes (NaN) reach
 // the ionic terms: they run on a finite u there, which keeps exp off its NaN
 // path, and the Laplacian / adjoint-stencil terms still make the result NaN.
@@ -143,10 +133,9 @@ __device__ __forceinline__ double finite_u(double u) {
 
 // Forward vector field at shared-memory cell q of a region W doubles wide with
 // field planes RN apart: 5-point Laplacian with NaN mirroring + F_ion + E*gh.
-// When J is non-null, J_F(y)^T of the cell goes there too (holes: unset).
 template <int W, int RN>
 __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restrict__ Y, int q,
-                                       double Egh, double& fu, double& fv, double& fw, JacT* J = nullptr) {
+                                       double Egh, double& fu, double& fv, double& fw) {
     const double u = Y[q];
 #if FKADJ_HOLE_BRANCH
     // holes and the NaN ring skip the arithmetic (their result is NaN either way)
@@ -170,12 +159,7 @@ __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restri
     const double lv = P.cv * ((((a_v + b_v) + c_v) + d_v) - 4.0 * v);
     const double lw = P.cw * ((((a_w + b_w) + c_w) + d_w) - 4.0 * w);
     double ud, vd, wd;
-    const double uf = finite_u(u);
-    Step sp, sq;
-    steps_pq(P, uf, sp, sq);
-    const Step ss = smooth_step(P.k_fk * (uf - P.u_csi));
-    fk_ion_from(P, uf, v, w, sp, sq, ss, ud, vd, wd);
-    if (J) *J = fk_jacT_from(P, uf, v, w, sp, sq, ss);  // the same steps: J_F(y)^T nearly for free
+    fk_ion(P, finite_u(u), v, w, ud, vd, wd);
     fu = (lu + ud) + Egh;
     fv = lv + vd;
     fw = lw + wd;

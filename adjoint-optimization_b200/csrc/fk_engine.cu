@@ -93,7 +93,7 @@ Problem::~Problem() {
 
 bool Problem::GraphKey::operator==(const GraphKey& o) const {
     if (policy != o.policy || nslots != o.nslots || seg_slots != o.seg_slots || keep_f != o.keep_f ||
-        keep_j != o.keep_j || exact != o.exact || gen != o.gen)
+        exact != o.exact || gen != o.gen)
         return false;
     for (int k = 0; k < 4; ++k)
         if (tk[k] != o.tk[k] || ty[k] != o.ty[k]) return false;
@@ -176,8 +176,8 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     for (auto& e : ev_) CK(cudaEventCreate(&e), "cudaEventCreate");
     if (pool_) {
         DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &work_,
-                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &kj_, &y0res_, &stg_,
-                         &jcache_, &fcache_, &Ed_};
+                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
+                         &fcache_, &Ed_};
         for (DevBuf* b : all) b->st = st_, b->pool = pool_;
     }
     {
@@ -299,7 +299,7 @@ int64_t Problem::estimate_bytes(int nrows, int ncols, int nt, int n_num, int64_t
 
 int64_t Problem::device_bytes() const {
     const DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_,
-                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &kj_, &y0res_, &stg_, &jcache_, &fcache_};
+                           &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_, &fcache_};
     int64_t s = 0;
     for (auto* b : all) s += (int64_t)b->bytes;
     return s;
@@ -400,9 +400,9 @@ void Problem::kernel_time(int k, double* avg_ms, int64_t* samples) const {
     if (samples) *samples = ksamples_[k];
 }
 
-fkadj_status Problem::step_forward(int i, const double* yin, double* yout, double* k1, double* j1) {
+fkadj_status Problem::step_forward(int i, const double* yin, double* yout, double* k1) {
     CK(prof_begin(K_FWD), "profiling event");
-    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), efwd(i), st_, nullptr, ty_[T_FWD], k1, j1),
+    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), efwd(i), st_, nullptr, ty_[T_FWD], k1),
        "forward step");
     CK(prof_end(K_FWD), "profiling event");
     ++launches_;
@@ -569,23 +569,19 @@ fkadj_status Problem::plan_trajectory(TrajPlan& tp) {
     if (grad_mode_ == FKADJ_GRAD_REF && pol != FKADJ_CKPT_BINOMIAL) {
         const double kslots = pol == FKADJ_CKPT_FULL ? (double)nt_ : (double)tp.seg_slots;
         tp.keep_f = need + kslots * sb <= (double)ckpt_budget_;
-        // and J_F(y)^T from the segment recompute (7 planes, 7/3 of a state each)
-        if (pol == FKADJ_CKPT_SQRT && tp.keep_f)
-            tp.keep_j = need + kslots * sb * (1.0 + 7.0 / 3.0) <= (double)ckpt_budget_;
     }
     return FKADJ_OK;
 }
 
 fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
     if (traj_.p && traj_plan_.policy == tp.policy && traj_plan_.nslots == tp.nslots &&
-        traj_plan_.seg_slots == tp.seg_slots && traj_plan_.keep_f == tp.keep_f && traj_plan_.keep_j == tp.keep_j)
+        traj_plan_.seg_slots == tp.seg_slots && traj_plan_.keep_f == tp.keep_f)
         return FKADJ_OK;
     drop_graph();
     ++buf_gen_;
     traj_.release();
     seg_.release();
     kf_.release();
-    kj_.release();
     CK(traj_.alloc((size_t)tp.nslots * state_bytes()), "alloc trajectory");
     CK(cudaMemsetAsync(traj_.p, 0xff, traj_.bytes, st_), "init trajectory");
     if (tp.seg_slots) {
@@ -597,10 +593,6 @@ fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
         const size_t k = tp.policy == FKADJ_CKPT_FULL ? (size_t)nt_ : (size_t)tp.seg_slots;
         CK(kf_.alloc(k * state_bytes()), "alloc kept f");
         CK(cudaMemsetAsync(kf_.p, 0xff, kf_.bytes, st_), "init kept f");
-    }
-    if (tp.keep_j) {
-        CK(kj_.alloc((size_t)tp.seg_slots * 7 * (size_t)g_.plane * sizeof(double)), "alloc kept J");
-        CK(cudaMemsetAsync(kj_.p, 0xff, kj_.bytes, st_), "init kept J");
     }
     traj_plan_ = tp;
     return FKADJ_OK;
@@ -935,8 +927,8 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
     // is valid only after a step that evaluated f(y_{i-1}) itself.
     bool have_fcarry = false, have_jcarry = false;
     int cur_c = 0;
-    auto back_step = [&](int i, const double* ya, const double* yb, const double* fa, const double* fb,
-                         const double* Ja = nullptr, const double* Jb = nullptr) -> fkadj_status {
+    auto back_step = [&](int i, const double* ya, const double* yb, const double* fa,
+                         const double* fb) -> fkadj_status {
         const int nxt = 1 - cur_c;
         const double* fin = fb ? fb : (have_fcarry ? fc[cur_c] : nullptr);
         CK(prof_begin(K_MID), "profiling event");
@@ -947,7 +939,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
                            gh_.as<double>(), prow(0, i - 1), nsbx_, st_,
-                           Jb ? Jb : (have_jcarry ? jy[cur_c] : nullptr), jh, jy[nxt], Ja),
+                           have_jcarry ? jy[cur_c] : nullptr, jh, jy[nxt]),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
@@ -955,7 +947,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         std::swap(z, z2);
         cur_c = nxt;
         have_fcarry = fa == nullptr;
-        have_jcarry = Ja == nullptr;  // evaluated and stored by the last stage
+        have_jcarry = true;
         return FKADJ_OK;
     };
     if (exact) {
@@ -991,17 +983,14 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
                 if (t == s1) return slot(k + 1);
                 return segslot(t - s0 - 1);
             };
-            // the recompute keeps f(y_t) (and J_F(y_t)^T) for t = s0 .. s1-2
+            // the recompute keeps f(y_t) for t = s0 .. s1-2 in fslot(t - s0)
             auto kept = [&](int t) -> double* {
                 return (tp.keep_f && t >= s0 && t <= s1 - 2) ? fslot(t - s0) : nullptr;
             };
-            auto keptJ = [&](int t) -> double* {
-                return (tp.keep_j && t >= s0 && t <= s1 - 2) ? jslot(t - s0) : nullptr;
-            };
             for (int t = s0; t < s1 - 1; ++t)
-                if ((s = step_forward(t, st(t), st(t + 1), kept(t), keptJ(t)))) return s;
+                if ((s = step_forward(t, st(t), st(t + 1), kept(t)))) return s;
             for (int i = s1; i > s0; --i)
-                if ((s = back_step(i, st(i - 1), st(i), kept(i - 1), kept(i), keptJ(i - 1), keptJ(i)))) return s;
+                if ((s = back_step(i, st(i - 1), st(i), kept(i - 1), kept(i)))) return s;
         }
     }
     const int rows = exact ? 3 * nt : nt + 1;
@@ -1016,7 +1005,6 @@ Problem::GraphKey Problem::graph_key(const TrajPlan& tp, bool exact) const {
     key.nslots = tp.nslots;
     key.seg_slots = tp.seg_slots;
     key.keep_f = tp.keep_f;
-    key.keep_j = tp.keep_j;
     key.exact = exact;
     key.gen = buf_gen_;
     for (int k = 0; k < 4; ++k) key.tk[k] = tk_[k], key.ty[k] = ty_[k];

@@ -63,7 +63,6 @@ struct TrajPlan {
     int seg_slots = 0;             // recompute buffer slots
     bool keep_f = false;           // k1 = f(y_t, Et[t]) kept beside the states the
                                    // backward sweep walks (FULL: all, SQRT: the segment)
-    bool keep_j = false;           // J_F(y_t)^T kept by the segment recompute (SQRT)
 };
 
 class BatchEngine;
@@ -124,7 +123,7 @@ public:
     // Spline samples of Et on the host; with upload, also the device tables the
     // standalone kernels read (the batched kernels take E by value).
     fkadj_status prepare_E(const double* Et, bool upload = true);
-    fkadj_status step_forward(int i, const double* yin, double* yout, double* k1 = nullptr, double* j1 = nullptr);
+    fkadj_status step_forward(int i, const double* yin, double* yout, double* k1 = nullptr);
     double* state_buf(int k) const { return work_.as<double>() + (size_t)k * state_elems(); }
     size_t state_elems() const { return (size_t)3 * g_.plane; }
     size_t state_bytes() const { return state_elems() * sizeof(double); }
@@ -158,7 +157,6 @@ private:
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
     double* segslot(int k) const { return seg_.as<double>() + (size_t)k * state_elems(); }
     double* fslot(int k) const { return kf_.as<double>() + (size_t)k * state_elems(); }
-    double* jslot(int k) const { return kj_.as<double>() + (size_t)k * 7 * g_.plane; }
     // E samples of step i read from the device tables (uploaded by prepare_E)
     const double* etab() const { return Ed_.as<double>(); }
     EStep efwd(int i) const {
@@ -202,7 +200,6 @@ private:
     DevBuf zgh_;       // nt+1
     DevBuf traj_, seg_;
     DevBuf kf_;        // kept k1 = f(y_t) per stored / recomputed state (TrajPlan::keep_f)
-    DevBuf kj_;        // kept J_F(y_t)^T per recomputed state (TrajPlan::keep_j), 7 planes each
     DevBuf y0res_;     // resident initial state
     DevBuf stg_;       // stage states Y2, Y3, Y4 of one step (exact mode)
     DevBuf jcache_;    // cached Jacobians (reference mode): J(y) ping-pong + J(yh)
@@ -215,7 +212,7 @@ private:
 
     // captured gradient sequence
     struct GraphKey {
-        int policy = -1, nslots = 0, seg_slots = 0, keep_f = 0, keep_j = 0, exact = 0, gen = 0;
+        int policy = -1, nslots = 0, seg_slots = 0, keep_f = 0, exact = 0, gen = 0;
         int tk[4] = {0, 0, 0, 0}, ty[4] = {0, 0, 0, 0};
         bool operator==(const GraphKey& o) const;
     };

@@ -145,7 +145,7 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
                                           const double* __restrict__ y0g, const double* __restrict__ ghs,
                                           int ld, long long plane, double Ev, double cY, double cD,
                                           double* __restrict__ out, double* __restrict__ stage_out, int rows,
-                                          double* __restrict__ k_out = nullptr, double* __restrict__ j_out = nullptr) {
+                                          double* __restrict__ k_out = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E;
     constexpr int IN = TX * TY;
@@ -159,19 +159,8 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
         const double gv = __ldg(ghs + o);
         const double a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
         double ku, kv, kw;
+        rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw);
         const bool inner = (E == 0) || (r >= HALO && r < HALO + rows && c >= HALO && c < HALO + TX);
-        JacT Jk;
-        const bool keepj = MODE == 0 && j_out && inner;
-        rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw, keepj ? &Jk : nullptr);
-        if (keepj && !isnan(src[s])) {  // J_F(y)^T, kept for the adjoint step
-            j_out[o] = Jk.a0;
-            j_out[plane + o] = Jk.a1;
-            j_out[2 * plane + o] = Jk.a2;
-            j_out[3 * plane + o] = Jk.a3;
-            j_out[4 * plane + o] = Jk.a4;
-            j_out[5 * plane + o] = Jk.a5;
-            j_out[6 * plane + o] = Jk.a6;
-        }
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
             out[o] = (a + D[d]) + cD * ku;
@@ -212,15 +201,13 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
 // in the last row of tiles is cut at the grid's edge).  When `stages` is
 // non-null the stage states Y2 = y + dt/2 k1, Y3 = y + dt/2 k2, Y4 = y + dt k3
 // are stored there too (three consecutive states), for the discrete-exact
-// adjoint; when `k1` is non-null, k1 = f(y, E0) is stored there (a state), and
-// when `j1` is non-null, J_F(y)^T (seven planes).  The tile functions may run several times per CTA (batched
+// adjoint; when `k1` is non-null, k1 = f(y, E0) is stored there (a state).  The tile functions may run several times per CTA (batched
 // kernels): they start by overwriting all the shared memory they read.
 template <int TX, int TY, int NT>
 __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ yin,
                                               double* __restrict__ yout, const double* __restrict__ gh, double E0,
                                               double Eh, double E1, double* __restrict__ stages, int tbx, int tby,
-                                              int ty, double* __restrict__ k1 = nullptr,
-                                              double* __restrict__ j1 = nullptr) {
+                                              int ty, double* __restrict__ k1 = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -241,7 +228,7 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     double* s3 = stages ? stages + sst + off : nullptr;
     double* s4 = stages ? stages + 2 * sst + off : nullptr;
     fwd_stage<3, TX, TY, NT, 0>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2,
-                                rows, k1 ? k1 + off : nullptr, j1 ? j1 + off : nullptr);
+                                rows, k1 ? k1 + off : nullptr);
     fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3,
                                 rows);
     fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4,
@@ -254,10 +241,9 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin, double* __restrict__ yout,
                const double* __restrict__ gh, EStep E, double* __restrict__ stages, int ty,
-               double* __restrict__ k1, double* __restrict__ j1) {
+               double* __restrict__ k1) {
     pdl_enter();
-    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1,
-                              j1);
+    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -465,9 +451,8 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
 // stages 2-3 the midpoint yh, stage 4 y(t_{i-1}) = ya; the tile's 16x16
 // sub-block sums of z_u . gh (NaN terms skipped, cu-G:1457-1483) go to `row`.
 // Jacobian caches (null = evaluate): jb = J(y_i) left by the previous step's
-// last stage, jh = J(yh) from k_adj_mid; J(y_{i-1}) is read from ja_in when the
-// forward recompute kept it, else evaluated in the last stage and stored to ja
-// for the next step.
+// last stage, jh = J(yh) from k_adj_mid; J(y_{i-1}) is evaluated in the last
+// stage and stored to ja for the next step.
 template <int TX, int TY, int NT>
 __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ z,
                                               double* __restrict__ zout, const double* __restrict__ yb,
@@ -475,7 +460,7 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
                                               const uint8_t* __restrict__ wc, const double* __restrict__ gh,
                                               double* __restrict__ row, int nsbx, const double* __restrict__ jb,
                                               const double* __restrict__ jh, double* __restrict__ ja, int tbx,
-                                              int tby, const double* __restrict__ ja_in = nullptr) {
+                                              int tby) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -490,8 +475,7 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
     adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb, nullptr);
     adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
     adj_stage<1, TX, TY, NT, 1>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
-    adj_stage<0, TX, TY, NT, 2>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, ja_in,
-                                ja_in ? nullptr : ja);
+    adj_stage<0, TX, TY, NT, 2>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, nullptr, ja);
     __syncthreads();
     subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
 }
@@ -501,11 +485,9 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z, double* __restrict__ zout,
                const double* __restrict__ yb, const double* __restrict__ yh, const double* __restrict__ ya,
                const uint8_t* __restrict__ wc, const double* __restrict__ gh, double* __restrict__ row, int nsbx,
-               const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja,
-               const double* __restrict__ ja_in) {
+               const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja) {
     pdl_enter();
-    adj_step_tile<TX, TY, NT>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y,
-                              ja_in);
+    adj_step_tile<TX, TY, NT>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------ exact-mode adjoint
@@ -935,13 +917,11 @@ static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
 }
 
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
-                            const double* gh, const EStep& E, cudaStream_t st, double* stages, int ty, double* k1,
-                            double* j1) {
+                            const double* gh, const EStep& E, cudaStream_t st, double* stages, int ty, double* k1) {
     DISPATCH(tile, {
         const int rows = (ty > 0 && ty < TY) ? ty : TY;
         const cudaError_t e = launch_pdl(k_fwd_step<TX, TY, NT>, tile_grid(g, TX, rows), NT,
-                                         stencil_smem<TX, TY>(NT), st, P, g, yin, yout, gh, E, stages, rows, k1,
-                                         j1);
+                                         stencil_smem<TX, TY>(NT), st, P, g, yin, yout, gh, E, stages, rows, k1);
         if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
@@ -1000,10 +980,10 @@ int balanced_rows(int tile, int kind, const DevGrid& g) {
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
                             const double* gh, double* row, int nsbx, cudaStream_t st, const double* jb,
-                            const double* jh, double* ja, const double* ja_in) {
+                            const double* jh, double* ja) {
     DISPATCH(tile, {
         const cudaError_t e = launch_pdl(k_adj_step<TX, TY, NT>, tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT),
-                                         st, P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, ja_in);
+                                         st, P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja);
         if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();

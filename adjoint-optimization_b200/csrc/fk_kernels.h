@@ -100,12 +100,11 @@ cudaError_t kernels_init();
 
 // ty: rows per tile, 0 < ty < the preset's height, or 0 for the preset's
 // height (forward step and adjoint midpoint only).  k1 (forward step): where
-// k1 = f(y, E0) is kept (a state, null = not kept); j1: where J_F(y)^T is kept
-// (seven planes, null = not kept).  fa (midpoint): f(ya, Ea)
+// k1 = f(y, E0) is kept (a state, null = not kept).  fa (midpoint): f(ya, Ea)
 // as kept by the forward step from ya (null = evaluate).
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
                             const double* gh, const EStep& E, cudaStream_t st, double* stages = nullptr, int ty = 0,
-                            double* k1 = nullptr, double* j1 = nullptr);
+                            double* k1 = nullptr);
 // Programmatic dependent launch for the step kernels issued by this thread
 // (on by default; the engine turns it off while it captures a graph).
 void set_launch_pdl(bool on);
@@ -125,12 +124,11 @@ cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const 
                            const double* fin = nullptr, double* fout = nullptr, double* jh = nullptr, int ty = 0,
                            const double* fa = nullptr);
 // jb: cached J(y_i) (null = evaluate), jh: cached J(yh) (null = evaluate),
-// ja: where J(y_{i-1}) is stored for the next step (null = not kept); ja_in:
-// J(y_{i-1}) kept by the forward recompute (then read, not evaluated or stored).
+// ja: where J(y_{i-1}) is stored for the next step (null = not kept).
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
                             const double* gh, double* row, int nsbx, cudaStream_t st, const double* jb = nullptr,
-                            const double* jh = nullptr, double* ja = nullptr, const double* ja_in = nullptr);
+                            const double* jh = nullptr, double* ja = nullptr);
 cudaError_t launch_dot_gh(const DevGrid& g, const double* z, const double* gh, double* row, int nsbx, int nsby,
                           cudaStream_t st);
 cudaError_t launch_sum_rows(const double* partial, int rows, int ntiles, double* out, cudaStream_t st);
