@@ -6,7 +6,8 @@
 // takes the next action of every active job and runs them as at most three
 // launches -- all forward-type steps, all midpoint steps, all adjoint steps of
 // every job -- through the batched persistent kernels (k_batch_*), whose work
-// queues go by value.  Jobs of different grid sizes and horizons therefore
+// queues reach the device in one small copy per tick.  Jobs of different grid
+// sizes and horizons therefore
 // share every launch, small grids fill the GPU together, and a job finishing or
 // starting changes only the next tick's queue.  The reference has no batching
 // (one instance per MATLAB call, simple_grad_desc.m:82).
