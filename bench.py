@@ -55,6 +55,9 @@ BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
 # halo) reach DRAM; the 24 B/cell of writes stay in the 126 MB L2.
 FWD_TRAFFIC_PER_CELL = 8656640 / 262144
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
+# discrete-exact adjoint step (--mode exact): read lambda (24), y (24), the three stage states (72), gh (8),
+# weight code (1); write lambda (24)
+EXACT_BYTES_PER_CELL = 153.0
 # FP64 flops per vector-field evaluation of the forward step (stage update included), counted by ncu
 # (2 x DFMA + DMUL + DADD thread instructions): profiles/fp64_ops_512x512.md
 FWD_FLOPS_PER_EVAL = 904.1 / 5.234375
@@ -133,9 +136,9 @@ def workload(args):
 
 def workload_config(args, inst, ckpt):
     return {"workload": f"FK {args.n}x{args.n} fp64, {args.nt} RK4 steps, 200 holes, 8 wavefronts, "
-                        f"400 E intervals, J=mean u^2, ref-mode adjoint, {ckpt} checkpoints",
+                        f"400 E intervals, J=mean u^2, {args.mode}-mode adjoint, {ckpt} checkpoints",
             "grid": [args.n, args.n], "nt": args.nt, "dt_ms": inst.dt, "dx_cm": inst.dx,
-            "active_cells": inst.n_num, "checkpoint": ckpt, "grad_mode": "ref",
+            "active_cells": inst.n_num, "checkpoint": ckpt, "grad_mode": args.mode,
             "l2": "working set larger than L2 (checkpoint + segment store > 1 GB per gradient)",
             "parallelism": f"replicas x{args.gpus}"}
 
@@ -235,7 +238,8 @@ def run_ours(args):
     inst = workload(args)
     ckpt = {"sqrt": _lib.CKPT_SQRT, "full": _lib.CKPT_FULL, "auto": _lib.CKPT_AUTO}[args.ckpt]
     stream = torch.cuda.Stream()
-    opts = api.options(ckpt_policy=ckpt, stream=stream.cuda_stream, device=local, tile=args.tile)
+    gmode = _lib.GRAD_EXACT if args.mode == "exact" else _lib.GRAD_REF
+    opts = api.options(ckpt_policy=ckpt, stream=stream.cuda_stream, device=local, tile=args.tile, grad_mode=gmode)
     pb = api.Problem(inst, opts=opts)
     Et = np.ascontiguousarray(inst.Et)
     pb.grad(Et, inst.y0)                     # uploads the initial state (resident afterwards)
@@ -263,22 +267,30 @@ def run_ours(args):
     pb.grad(Et)
     pb.set_profiling(False)
     recompute = 0 if args.ckpt == "full" else inst.nt - (inst.nt + pb_stride(inst.nt) - 1) // pb_stride(inst.nt)
-    per_grad = {0: inst.nt + recompute, 1: inst.nt, 2: inst.nt}
-    kt = {k: pb.kernel_time(k) for k in (0, 1, 2)}
+    names, nbytes = dict(KERNEL_NAMES), dict(BYTES_PER_CELL)
+    if args.mode == "exact":
+        # forward sweep + recompute + one stage replay per backward step; the
+        # discrete adjoint step in the adjoint slot; no midpoint kernel
+        per_grad = {0: 2 * inst.nt + recompute, 2: inst.nt}
+        names[2], nbytes[2] = "k_adj_exact", EXACT_BYTES_PER_CELL
+    else:
+        per_grad = {0: inst.nt + recompute, 1: inst.nt, 2: inst.nt}
+    kt = {k: pb.kernel_time(k) for k in per_grad}
     tiles = pb.tiles
     share = {k: kt[k][0] * per_grad[k] for k in kt}
     dom = max(share, key=share.get)
     cells = inst.nrows * inst.ncols
     avg_ms = kt[dom][0]
-    achieved = BYTES_PER_CELL[dom] * cells / (avg_ms / 1000.0) / 1e9
+    achieved = nbytes[dom] * cells / (avg_ms / 1000.0) / 1e9
     peak, peak_kind = peaks()
-    roof = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roof = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind, "traffic": args.traffic,
-            "bytes_per_launch": BYTES_PER_CELL[dom] * cells, "avg_launch_ms": avg_ms,
+            "bytes_per_launch": nbytes[dom] * cells, "avg_launch_ms": avg_ms,
             "samples": kt[dom][1],
-            "kernel_ms": {KERNEL_NAMES[k]: kt[k][0] for k in kt},
-            "time_share": {KERNEL_NAMES[k]: share[k] / sum(share.values()) for k in share},
-            "tiles": {k: list(v) for k, v in tiles.items() if k != "adj_exact"},
+            "kernel_ms": {names[k]: kt[k][0] for k in kt},
+            "time_share": {names[k]: share[k] / sum(share.values()) for k in share},
+            "tiles": {k: list(v) for k, v in tiles.items()
+                      if (k == "adj_exact") == (args.mode == "exact") or k == "fwd_step"},
             "note": "FP64 bound: a vector-field evaluation costs 2 exp, 3 reciprocals, 1 divide and ~60 "
                     "FMA-class operations, 4.6 evaluations per cell-step; the HBM fraction is reported "
                     "against the copy peak"}
@@ -301,7 +313,8 @@ def run_ours(args):
     full = None
     if not args.no_full and args.ckpt != "full" and world == 1:
         try:
-            fopts = api.options(ckpt_policy=_lib.CKPT_FULL, stream=stream.cuda_stream, device=local, tile=args.tile)
+            fopts = api.options(ckpt_policy=_lib.CKPT_FULL, stream=stream.cuda_stream, device=local, tile=args.tile,
+                                grad_mode=gmode)
             with api.Problem(inst, opts=fopts) as pf:
                 pf.grad(Et, inst.y0)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -326,7 +339,7 @@ def run_ours(args):
     h2d = Et_h.nbytes + y0_h.nbytes + ai_h.nbytes + gh_h.nbytes + 24 + S.indptr.size * 8 + S.indices.size * 8 \
         + S.data.size * 8
     d2h = (inst.nt + 1) * 8 + 3 * 8
-    eopts = api.options(ckpt_policy=ckpt, device=local, tile=args.tile)
+    eopts = api.options(ckpt_policy=ckpt, device=local, tile=args.tile, grad_mode=gmode)
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     barrier()
     t0 = time.perf_counter()
@@ -369,6 +382,8 @@ def main():
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--nt", type=int, default=20000)
     ap.add_argument("--ckpt", default="sqrt", choices=["sqrt", "full", "auto"])
+    ap.add_argument("--mode", default="ref", choices=["ref", "exact"],
+                    help="gradient mode: the reference's continuous adjoint (the headline) or the discrete-exact one")
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cpu-steps", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=3)
