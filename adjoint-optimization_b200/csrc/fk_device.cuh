@@ -186,7 +186,8 @@ __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restri
     const double vn = Y[RN + q - W], vs = Y[RN + q + W], vw = Y[RN + q - 1], ve = Y[RN + q + 1];
     const double wn = Y[2 * RN + q - W], ws = Y[2 * RN + q + W], ww = Y[2 * RN + q - 1],
                  we = Y[2 * RN + q + 1];
-    // neighbour pairs after mirroring (cu-F:319-420)
+    // neighbour pairs after mirroring (cu-F:319-420); selects, not a branch to
+    // a plain sum away from holes, which measured 4 % slower on the forward step
     const double a_u = nN ? us : un, b_u = nS ? un : us, c_u = nW ? ue : uw, d_u = nE ? uw : ue;
     const double a_v = nN ? vs : vn, b_v = nS ? vn : vs, c_v = nW ? ve : vw, d_v = nE ? vw : ve;
     const double a_w = nN ? ws : wn, b_w = nS ? wn : ws, c_w = nW ? we : ww, d_w = nE ? ww : we;
