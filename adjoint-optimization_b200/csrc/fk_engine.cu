@@ -381,6 +381,16 @@ cudaError_t Problem::prof_end(int k) {
     return cudaEventRecord(prof_pool_[prof_used_++].b, st_);
 }
 
+fkadj_status Problem::check_fault() {
+    unsigned f = 0;
+    CK(take_device_fault(st_, &f), "read the device fault flag");
+    if (f) {
+        set_error("a bounded wait in a kernel expired (tile copy into shared memory); results are invalid");
+        return FKADJ_ERR_TIMEOUT;
+    }
+    return FKADJ_OK;
+}
+
 fkadj_status Problem::prof_collect() {
     if (!prof_used_) return FKADJ_OK;
     CK(cudaStreamSynchronize(st_), "synchronize");
@@ -453,6 +463,7 @@ fkadj_status Problem::forward(const double* Et, const double* y_ini, int nstep, 
         if ((s = download_grid(cur, yf))) return s;
     }
     CK(cudaStreamSynchronize(st_), "synchronize");
+    if ((s = check_fault())) return s;
     if ((s = prof_collect())) return s;
     float a = 0;
     cudaEventElapsedTime(&a, ev_[0], ev_[1]);
@@ -517,6 +528,7 @@ fkadj_status Problem::objective(const double* Et, const double* y_ini, double* L
     if (Lcost) *Lcost = 0.5 * l0 + 0.5 * alpha_ * le;
     if (yf && (s = download_grid(cur, yf))) return s;
     CK(cudaStreamSynchronize(st_), "synchronize");
+    if ((s = check_fault())) return s;
     if ((s = prof_collect())) return s;
     float a = 0, b = 0;
     cudaEventElapsedTime(&a, ev_[0], ev_[1]);
@@ -1102,6 +1114,7 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     if ((s = replay ? grad_replay(tp, exact, &yT) : grad_sequence(tp, exact, &yT))) return s;
     if (yf && (s = download_grid(yT, yf))) return s;
     CK(cudaStreamSynchronize(st_), "synchronize");
+    if ((s = check_fault())) return s;
     if ((s = prof_collect())) return s;
     const double l0 = -hres_[0];
     const double* zgh = hres_ + 1;

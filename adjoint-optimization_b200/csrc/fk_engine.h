@@ -134,6 +134,8 @@ private:
     cudaError_t prof_begin(int k);
     cudaError_t prof_end(int k);
     fkadj_status prof_collect();
+    // FKADJ_ERR_TIMEOUT when a kernel's bounded wait expired since the last check
+    fkadj_status check_fault();
     fkadj_status plan_trajectory(TrajPlan& tp);
     fkadj_status ensure_traj(const TrajPlan& tp);
     fkadj_status run_objective(const double* yT, double* L0);

@@ -48,6 +48,10 @@ __device__ __forceinline__ void pdl_enter() {
 // little but keep two or three CTAs per SM, which measured faster: 32 x 128^2
 // batched 0.58 s against 0.71 s, 16 x 256^2 0.48 s against 0.72 s), or 1 (no
 // spills).
+#ifndef FKADJ_LOAD_UNROLL
+#define FKADJ_LOAD_UNROLL 4
+#endif
+constexpr int kLoadUnroll = FKADJ_LOAD_UNROLL;
 #ifndef FKADJ_BATCH_ONE_CTA
 #define FKADJ_BATCH_ONE_CTA 0
 #endif
@@ -86,7 +90,7 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
     if (vec_ok && (WIDTH % 2) == 0) {
         constexpr int HW = WIDTH / 2;
         const int per = rows * HW;
-#pragma unroll 2
+#pragma unroll kLoadUnroll
         for (int q = threadIdx.x; q < 3 * per; q += NT) {
             const int f = q >= per ? (q >= 2 * per ? 2 : 1) : 0;
             const int rem = q - f * per;
@@ -96,7 +100,7 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
         }
     } else {
         const int per = rows * WIDTH;
-#pragma unroll 2
+#pragma unroll kLoadUnroll
         for (int q = threadIdx.x; q < 3 * per; q += NT) {
             const int f = q >= per ? (q >= 2 * per ? 2 : 1) : 0;
             const int rem = q - f * per;
@@ -104,6 +108,103 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
             dst[f * RN + r * WIDTH + c] = __ldg(src + f * plane + (long long)r * ld + c);
         }
     }
+}
+
+// Set when a bounded wait in a kernel gave up (read and cleared by the host
+// after each call: take_device_fault).
+__device__ unsigned int g_device_fault = 0;
+
+// Tile loads through the bulk-copy (TMA) engine: one cp.async.bulk per row and
+// field of the window load_region copies, completing on an mbarrier in shared
+// memory.  Used by the one-tile-per-CTA step kernels when the window starts on
+// an even column: every row then starts on a 16-byte boundary (ld and the
+// plane pitch are multiples of 8 doubles) and is WIDTH * 8 bytes long, a
+// multiple of 16.  The waits are bounded; on expiry g_device_fault is set.
+#ifndef FKADJ_BULK_LOAD
+#define FKADJ_BULK_LOAD 1
+#endif
+
+// Shared-memory address of the CTA's mbarrier, initialised by thread 0 for one
+// arrival; the caller synchronises the CTA before its first use.
+__device__ __forceinline__ uint32_t bulk_begin(uint64_t* bar) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    return a;
+}
+
+// Bytes of a rows x WIDTH window of the three planes.
+template <int WIDTH>
+__device__ __forceinline__ uint32_t bulk_bytes(int rows) {
+    static_assert((WIDTH * 8) % 16 == 0, "bulk rows must be 16-byte multiples");
+    return 3u * (uint32_t)rows * WIDTH * 8u;
+}
+
+// Thread 0 arrives on the barrier with the transfer's byte count; the CTA
+// synchronises before the copies are issued.
+__device__ __forceinline__ void bulk_arrive(uint32_t bar, uint32_t bytes) {
+    if (threadIdx.x == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Issues the copies of one window (the load_region window: row pitch WIDTH,
+// plane pitch RCAP * WIDTH in shared memory), spread over the threads.
+template <int RCAP, int WIDTH, int NT>
+__device__ __forceinline__ void bulk_issue(uint32_t bar, double* dst, const double* src, int ld, long long plane,
+                                           int rows) {
+    constexpr int RN = RCAP * WIDTH;
+    for (int t = threadIdx.x; t < 3 * rows; t += NT) {
+        const int f = t / rows, r = t - f * rows;
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + f * RN + r * WIDTH);
+        const size_t gsrc = __cvta_generic_to_global(src + f * plane + (long long)r * ld);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+            "l"(gsrc), "n"(WIDTH * 8), "r"(bar)
+            : "memory");
+    }
+}
+
+// Waits for phase 0 of the barrier, at most about 2^20 polls (each poll may
+// suspend the thread briefly); records an expired wait in g_device_fault.
+__device__ __forceinline__ void bulk_wait(uint32_t bar) {
+    for (int it = 0; it < (1 << 20); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+        if (done) return;
+    }
+    atomicOr(&g_device_fault, 1u);
+}
+
+// Copies one window (d1 null) or two windows of the same shape into shared
+// memory: through the bulk-copy engine when BULK and the windows start on an
+// even column, else with vector loads.  Ends with the CTA synchronised.
+template <int RCAP, int WIDTH, int NT, bool BULK>
+__device__ __forceinline__ void load_windows(double* __restrict__ d0, const double* __restrict__ s0,
+                                             double* __restrict__ d1, const double* __restrict__ s1, int ld,
+                                             long long plane, bool vec_ok, int rows) {
+    // every row start 16-byte aligned, checked on the addresses themselves
+    const bool aligned = vec_ok && ((reinterpret_cast<uintptr_t>(s0) | reinterpret_cast<uintptr_t>(s1) |
+                                     (uintptr_t)ld * 8u | (uintptr_t)plane * 8u) & 15) == 0;
+    if (BULK && FKADJ_BULK_LOAD && aligned) {
+        __shared__ uint64_t bar;
+        const uint32_t b = bulk_begin(&bar);
+        __syncthreads();
+        bulk_arrive(b, bulk_bytes<WIDTH>(rows) * (d1 ? 2u : 1u));
+        __syncthreads();
+        bulk_issue<RCAP, WIDTH, NT>(b, d0, s0, ld, plane, rows);
+        if (d1) bulk_issue<RCAP, WIDTH, NT>(b, d1, s1, ld, plane, rows);
+        bulk_wait(b);
+    } else {
+        load_region<RCAP, WIDTH, NT>(d0, s0, ld, plane, vec_ok, rows);
+        if (d1) load_region<RCAP, WIDTH, NT>(d1, s1, ld, plane, vec_ok, rows);
+    }
+    __syncthreads();
 }
 
 // Fixed-order block sum (warp shuffles, then warps in order); result valid in
@@ -220,7 +321,7 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
 // are stored there too (three consecutive states), for the discrete-exact
 // adjoint; when `k1` is non-null, k1 = f(y, E0) is stored there (a state).  The tile functions may run several times per CTA (batched
 // kernels): they start by overwriting all the shared memory they read.
-template <int TX, int TY, int NT>
+template <int TX, int TY, int NT, bool BULK = false>
 __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ yin,
                                               double* __restrict__ yout, const double* __restrict__ gh, double E0,
                                               double Eh, double E1, double* __restrict__ stages, int tbx, int tby,
@@ -235,8 +336,7 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     // region origin: logical (i0 - HALO, j0 - HALO) = padded (i0, j0)
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(A, yin + off, g.ld, g.plane, vec_ok, rows + 2 * HALO);
-    __syncthreads();
+    load_windows<RH, RW, NT, BULK>(A, yin + off, nullptr, nullptr, g.ld, g.plane, vec_ok, rows + 2 * HALO);
     const double* y0g = yin + off;
     const double* ghs = gh + off;
     const double dt = P.dt;
@@ -260,7 +360,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                const double* __restrict__ gh, EStep E, double* __restrict__ stages, int ty,
                double* __restrict__ k1) {
     pdl_enter();
-    fwd_step_tile<TX, TY, NT>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1);
+    fwd_step_tile<TX, TY, NT, true>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -297,7 +397,7 @@ __device__ __forceinline__ void store_jac(double* __restrict__ Jb, long long pla
 //   f(ya, Ea) is k1 of the forward step from ya: when fa is non-null (the
 //   forward recompute kept it) it is read from there too;
 //   J_F(yh)^T, used by stages 2 and 3 of the adjoint step, goes to jh.
-template <int TX, int TY, int NT>
+template <int TX, int TY, int NT, bool BULK = false>
 __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ ya,
                                              const double* __restrict__ yb, const double* __restrict__ gh,
                                              double* __restrict__ yh, double Ea, double Eb, double E3,
@@ -315,9 +415,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
     // region origin: logical (i0 - 2, j0 - 2) = padded (i0 + 2, j0 + 2)
     const long long off = (long long)(i0 + HALO - H2) * g.ld + (j0 + HALO - H2);
     const bool vec_ok = ((g.ld | (j0 + HALO - H2)) & 1) == 0;
-    load_region<RH, RW, NT>(A, ya + off, g.ld, g.plane, vec_ok, rows + 2 * H2);
-    load_region<RH, RW, NT>(B, yb + off, g.ld, g.plane, vec_ok, rows + 2 * H2);
-    __syncthreads();
+    load_windows<RH, RW, NT, BULK>(A, ya + off, B, yb + off, g.ld, g.plane, vec_ok, rows + 2 * H2);
     const double dt = P.dt;
     {
         constexpr int W = TX + 2;
@@ -390,7 +488,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
               const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty,
               const double* __restrict__ fa) {
     pdl_enter();
-    adj_mid_tile<TX, TY, NT>(P, g, ya, yb, gh, yh, E.a(), E.b(), E.c(), hw, fin, fout, jh, blockIdx.x, blockIdx.y,
+    adj_mid_tile<TX, TY, NT, true>(P, g, ya, yb, gh, yh, E.a(), E.b(), E.c(), hw, fin, fout, jh, blockIdx.x, blockIdx.y,
                              ty, fa);
 }
 
@@ -473,7 +571,7 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
 // Jacobian caches (null = evaluate): jb = J(y_i) left by the previous step's
 // last stage, jh = J(yh) from k_adj_mid; J(y_{i-1}) is evaluated in the last
 // stage and stored to ja for the next step.
-template <int TX, int TY, int NT>
+template <int TX, int TY, int NT, bool BULK = false>
 __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ z,
                                               double* __restrict__ zout, const double* __restrict__ yb,
                                               const double* __restrict__ yh, const double* __restrict__ ya,
@@ -489,8 +587,7 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(A, z + off, g.ld, g.plane, vec_ok, RH);
-    __syncthreads();
+    load_windows<RH, RW, NT, BULK>(A, z + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH);
     const double dt = P.dt;
     adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb, nullptr);
     adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
@@ -507,7 +604,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                const uint8_t* __restrict__ wc, const double* __restrict__ gh, double* __restrict__ row, int nsbx,
                const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja) {
     pdl_enter();
-    adj_step_tile<TX, TY, NT>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y);
+    adj_step_tile<TX, TY, NT, true>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------ exact-mode adjoint
@@ -580,7 +677,7 @@ __device__ __forceinline__ void exact_stage(const DevModel& P, const DevGrid& g,
 // lam (state of lambda_{s+1}) -> lamout (lambda_s); y = y_s; stages = Y2, Y3,
 // Y4 of step s (three consecutive states, written by k_fwd_step).
 // 16x16 sub-block sums: r1 <- b.a1, r23 <- b.(a2 + a3), r4 <- b.a4.
-template <int TX, int TY, int NT>
+template <int TX, int TY, int NT, bool BULK = false>
 __device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ lam,
                                                double* __restrict__ lamout, const double* __restrict__ y,
                                                const double* __restrict__ stages, const uint8_t* __restrict__ wc,
@@ -597,8 +694,7 @@ __device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid&
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_region<RH, RW, NT>(A, lam + off, g.ld, g.plane, vec_ok, RH);
-    __syncthreads();
+    load_windows<RH, RW, NT, BULK>(A, lam + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH);
     const double dt = P.dt;
     const double c6 = dt / 6.0, c3 = dt / 3.0, c2 = dt * 0.5;
 #pragma unroll 2
@@ -632,7 +728,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                 const double* __restrict__ gh, double* __restrict__ r1, double* __restrict__ r23,
                 double* __restrict__ r4, int nsbx) {
     pdl_enter();
-    adj_exact_tile<TX, TY, NT>(P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx, blockIdx.x, blockIdx.y);
+    adj_exact_tile<TX, TY, NT, true>(P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- batched
@@ -877,6 +973,19 @@ TileShape tile_shape(int t) {
 #undef X
         default: return {32, 32, 256};
     }
+}
+
+cudaError_t take_device_fault(cudaStream_t st, unsigned* fault) {
+    unsigned v = 0;
+    cudaError_t e = cudaMemcpyFromSymbolAsync(&v, g_device_fault, sizeof v, 0, cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    if (!e && v) {
+        const unsigned zero = 0;
+        e = cudaMemcpyToSymbolAsync(g_device_fault, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, st);
+        if (!e) e = cudaStreamSynchronize(st);
+    }
+    *fault = v;
+    return e;
 }
 
 cudaError_t kernels_init() {

@@ -97,6 +97,9 @@ int batch_preset(int tile);
 TileShape tile_shape(int tile);
 int tiles_of(int tile, const DevGrid& g);
 cudaError_t kernels_init();
+// Reads and clears the flag a kernel sets when one of its bounded waits
+// expires (after synchronising st); *fault != 0 means results are invalid.
+cudaError_t take_device_fault(cudaStream_t st, unsigned* fault);
 
 // ty: rows per tile, 0 < ty < the preset's height, or 0 for the preset's
 // height (forward step and adjoint midpoint only).  k1 (forward step): where
