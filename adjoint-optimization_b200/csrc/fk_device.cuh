@@ -215,16 +215,16 @@ __device__ __forceinline__ void adj_at(const DevModel& P, const double* __restri
                                        int code, const JacT& J, double& gu, double& gv,
                                        double& gw) {
     const double z0 = Z[q], z1 = Z[RN + q], z2 = Z[2 * RN + q];
-    const double pn = (double)wcode_n(code), ps = (double)wcode_s(code);
-    const double pw = (double)wcode_w(code), pe = (double)wcode_e(code);
+    const int cn = wcode_n(code), cs = wcode_s(code), cw = wcode_w(code), ce = wcode_e(code);
+    const double pn = (double)cn, ps = (double)cs, pw = (double)cw, pe = (double)ce;
     double l[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
         const double* Zf = Z + f * RN;
-        const double vn = pn != 0.0 ? Zf[q - W] : 0.0;
-        const double vs = ps != 0.0 ? Zf[q + W] : 0.0;
-        const double vw = pw != 0.0 ? Zf[q - 1] : 0.0;
-        const double ve = pe != 0.0 ? Zf[q + 1] : 0.0;
+        const double vn = cn ? Zf[q - W] : 0.0;  // integer tests: no FP64 compares
+        const double vs = cs ? Zf[q + W] : 0.0;
+        const double vw = cw ? Zf[q - 1] : 0.0;
+        const double ve = ce ? Zf[q + 1] : 0.0;
         const double c = f == 0 ? P.cu : (f == 1 ? P.cv : P.cw);
         l[f] = c * ((((pn * vn + ps * vs) + pw * vw) + pe * ve) - 4.0 * Zf[q]);
     }
