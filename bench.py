@@ -263,7 +263,7 @@ def run_ours(args):
     value = replica_value(world, args.steps, ms)
     # the last timed gradient's forward sweep: CUDA events on the engine stream around its nt back-to-back
     # k_fwd_step launches (recorded inside the replayed graph)
-    fwd_sweep_ms = pb.last_timing()["fwd_ms"]
+    fwd_sweep_ms = pb.last_timing["fwd_ms"]
 
     # roofline: sampled per-kernel device times in one more gradient
     pb.set_profiling(True)
