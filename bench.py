@@ -60,7 +60,7 @@ KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
 EXACT_BYTES_PER_CELL = 153.0
 # FP64 flops per vector-field evaluation of the forward step (stage update included), counted by ncu
 # (2 x DFMA + DMUL + DADD thread instructions): profiles/fp64_ops_512x512.md
-FWD_FLOPS_PER_EVAL = 904.1 / 5.234375
+FWD_FLOPS_PER_EVAL = 740.4 / 4.58984375
 
 
 def fwd_evaluations(nrows, ncols, tx, ty):
@@ -299,7 +299,7 @@ def run_ours(args):
             "time_share": {names[k]: share[k] / sum(share.values()) for k in share},
             "tiles": {k: list(v) for k, v in tiles.items()
                       if (k == "adj_exact") == (args.mode == "exact") or k == "fwd_step"},
-            "note": "FP64 bound: a vector-field evaluation costs 2 exp, 3 reciprocals, 1 divide and ~60 "
+            "note": "FP64 bound: a vector-field evaluation costs 2 exp, 4 reciprocals and ~60 "
                     "FMA-class operations, 4.6 evaluations per cell-step; the HBM fraction is reported "
                     "against the copy peak"}
     # the forward step against the FP64 roof (the bound it is nearer to)
