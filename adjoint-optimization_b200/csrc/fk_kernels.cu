@@ -17,6 +17,7 @@
 // occupying shared memory, and the interior accumulator is the only other
 // shared buffer.
 #include "fk_kernels.h"
+#include "fk_bulk.cuh"
 
 #include <cstdio>
 #include <cstdlib>
@@ -114,72 +115,11 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
 // after each call: take_device_fault).
 __device__ unsigned int g_device_fault = 0;
 
-// Tile loads through the bulk-copy (TMA) engine: one cp.async.bulk per row and
-// field of the window load_region copies, completing on an mbarrier in shared
-// memory.  Used by the one-tile-per-CTA step kernels when the window starts on
-// an even column: every row then starts on a 16-byte boundary (ld and the
-// plane pitch are multiples of 8 doubles) and is WIDTH * 8 bytes long, a
-// multiple of 16.  The waits are bounded; on expiry g_device_fault is set.
+// Tile loads through the bulk-copy engine (fk_bulk.cuh) in the one-tile-per-CTA
+// step kernels; FKADJ_BULK_LOAD=0 keeps the vector loads everywhere.
 #ifndef FKADJ_BULK_LOAD
 #define FKADJ_BULK_LOAD 1
 #endif
-
-// Shared-memory address of the CTA's mbarrier, initialised by thread 0 for one
-// arrival; the caller synchronises the CTA before its first use.
-__device__ __forceinline__ uint32_t bulk_begin(uint64_t* bar) {
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    return a;
-}
-
-// Bytes of a rows x WIDTH window of the three planes.
-template <int WIDTH>
-__device__ __forceinline__ uint32_t bulk_bytes(int rows) {
-    static_assert((WIDTH * 8) % 16 == 0, "bulk rows must be 16-byte multiples");
-    return 3u * (uint32_t)rows * WIDTH * 8u;
-}
-
-// Thread 0 arrives on the barrier with the transfer's byte count; the CTA
-// synchronises before the copies are issued.
-__device__ __forceinline__ void bulk_arrive(uint32_t bar, uint32_t bytes) {
-    if (threadIdx.x == 0)
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-// Issues the copies of one window (the load_region window: row pitch WIDTH,
-// plane pitch RCAP * WIDTH in shared memory), spread over the threads.
-template <int RCAP, int WIDTH, int NT>
-__device__ __forceinline__ void bulk_issue(uint32_t bar, double* dst, const double* src, int ld, long long plane,
-                                           int rows) {
-    constexpr int RN = RCAP * WIDTH;
-    for (int t = threadIdx.x; t < 3 * rows; t += NT) {
-        const int f = t / rows, r = t - f * rows;
-        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + f * RN + r * WIDTH);
-        const size_t gsrc = __cvta_generic_to_global(src + f * plane + (long long)r * ld);
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
-            "l"(gsrc), "n"(WIDTH * 8), "r"(bar)
-            : "memory");
-    }
-}
-
-// Waits for phase 0 of the barrier, at most about 2^20 polls (each poll may
-// suspend the thread briefly); records an expired wait in g_device_fault.
-__device__ __forceinline__ void bulk_wait(uint32_t bar) {
-    for (int it = 0; it < (1 << 20); ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(done)
-            : "r"(bar)
-            : "memory");
-        if (done) return;
-    }
-    atomicOr(&g_device_fault, 1u);
-}
 
 // Copies one window (d1 null) or two windows of the same shape into shared
 // memory: through the bulk-copy engine when BULK and the windows start on an
@@ -199,7 +139,7 @@ __device__ __forceinline__ void load_windows(double* __restrict__ d0, const doub
         __syncthreads();
         bulk_issue<RCAP, WIDTH, NT>(b, d0, s0, ld, plane, rows);
         if (d1) bulk_issue<RCAP, WIDTH, NT>(b, d1, s1, ld, plane, rows);
-        bulk_wait(b);
+        if (!bulk_wait(b)) atomicOr(&g_device_fault, 1u);
     } else {
         load_region<RCAP, WIDTH, NT>(d0, s0, ld, plane, vec_ok, rows);
         if (d1) load_region<RCAP, WIDTH, NT>(d1, s1, ld, plane, vec_ok, rows);
