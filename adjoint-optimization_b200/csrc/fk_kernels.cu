@@ -213,9 +213,15 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
         const int r = rc.r, c = rc.c;
         const int s = r * RW + c;
         const long long o = (long long)r * ld + c;
-        // global operands first: their latency overlaps the stencil arithmetic
+        // global operands first: their latency overlaps the stencil arithmetic; the
+        // first stage's source region is the step-start state itself
         const double gv = __ldg(ghs + o);
-        const double a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
+        double a, b, e;
+        if (MODE == 0) {
+            a = src[s], b = src[RN + s], e = src[2 * RN + s];
+        } else {
+            a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
+        }
         double ku, kv, kw;
         rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw);
         const bool inner = (E == 0) || (r >= HALO && r < HALO + rows && c >= HALO && c < HALO + TX);
@@ -458,7 +464,12 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
         const int r = rc.r, c = rc.c;
         const int s = r * RW + c;
         const long long o = off + (long long)r * g.ld + c;
-        const double a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
+        double a, b, e;
+        if (MODE == 0) {  // the first stage's source region is z0 itself
+            a = src[s], b = src[RN + s], e = src[2 * RN + s];
+        } else {
+            a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
+        }
         const int code = __ldg(wc + o);
         double ku, kv, kw;
 #if FKADJ_HOLE_BRANCH
