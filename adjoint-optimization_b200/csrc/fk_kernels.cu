@@ -356,6 +356,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
     double* A = reinterpret_cast<double*>(smem_raw);
     double* B = A + 3 * RN;
     double* C = B + 3 * RN;
+    double* Q = C + 3 * RN;  // quartic part of yh on the tile, kept between the two loops
     const int i0 = tby * ty, j0 = tbx * TX;
     const int rows = min(ty, g.nrows - i0);
     // region origin: logical (i0 - 2, j0 - 2) = padded (i0 + 2, j0 + 2)
@@ -399,8 +400,10 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
                 const double m0 = a0[f] * dt, m1 = a1[f] * dt;
                 const double x0 = A[f * RN + s], x1 = B[f * RN + s];
                 C[f * RN + s] = ((hw.c3[0] * x0 + hw.c3[1] * m0) + hw.c3[2] * x1) + hw.c3[3] * m1;
-                if (inner)
-                    yh[o + f * g.plane] = ((hw.c4[0] * x0 + hw.c4[1] * m0) + hw.c4[2] * x1) + hw.c4[3] * m1;
+                if (inner) {
+                    Q[f * TX * TY + (r - H2) * TX + (c - H2)] =
+                        ((hw.c4[0] * x0 + hw.c4[1] * m0) + hw.c4[2] * x1) + hw.c4[3] * m1;
+                }
             }
         }
     }
@@ -419,7 +422,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
 #pragma unroll
             for (int f = 0; f < 3; ++f) {
                 double* p = yh + o + f * g.plane;
-                yv[f] = *p + hw.c2 * (m2[f] * dt);
+                yv[f] = Q[f * TX * TY + (r - H2) * TX + (c - H2)] + hw.c2 * (m2[f] * dt);
                 *p = yv[f];
             }
             if (jh && !isnan(yv[0])) store_jac(jh, g.plane, o, fk_jacT(P, yv[0], yv[1], yv[2]));
@@ -842,10 +845,12 @@ static size_t exact_smem() {
     constexpr int RN = (TX + 2 * HALO) * (TY + 2 * HALO);
     return sizeof(double) * (6 * RN + 4 * TX * TY);
 }
+// windows of y_{i-1}, y_i and y(1/3) on the tile + 2, and the quartic part of
+// yh on the tile (225 KB at 64x32)
 template <int TX, int TY>
 static size_t mid_smem() {
     constexpr int RN = (TX + 4) * (TY + 4);
-    return sizeof(double) * (9 * RN);
+    return sizeof(double) * (9 * RN + 3 * TX * TY);
 }
 
 template <int TX, int TY, int NT>
