@@ -78,6 +78,14 @@ static std::mutex g_init_mu;
 static bool g_init_done[64];
 
 Problem::~Problem() {
+    if (pool_) {
+        // stream-ordered frees need the stream (the problem's own one is destroyed
+        // below): release the buffers first
+        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &work_,
+                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
+                         &fcache_, &Ed_};
+        for (DevBuf* b : all) b->release();
+    }
     for (auto& r : prof_pool_) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -188,6 +196,12 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     }
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+    if (pool_) {  // memory the pool holds but no buffer uses is free for this problem too
+        uint64_t reserved = 0, used = 0;
+        if (cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+            cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+            fr += (size_t)(reserved - used);
+    }
     ckpt_budget_ = o.ckpt_budget_bytes > 0 ? o.ckpt_budget_bytes : (int64_t)(0.6 * (double)fr);
 
     g_.nrows = nrows;
