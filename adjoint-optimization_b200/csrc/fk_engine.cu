@@ -8,10 +8,12 @@
 #include "fk_engine.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -77,7 +79,100 @@ static inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 static std::mutex g_init_mu;
 static bool g_init_done[64];
 
+// The one-shot entry points (fkadj_grad, fkadj_forward) build a problem per
+// call.  Freeing its memory at the end of every call cost a call up to 0.8 s at
+// times (cudaFree of the trajectory store, cudaFreeHost of the pinned staging,
+// measured on B200), so one-shot problems keep both for the next call:
+//  - device memory from a stream-ordered pool per device that keeps what is
+//    freed (FKADJ_ONESHOT_POOL=0 in the environment: cudaMalloc instead);
+//  - pinned host staging from a small process-wide free list.
+// fkadj_release_cached_memory() hands both back.
+static std::mutex g_oneshot_mu;
+static cudaMemPool_t g_oneshot_pool[64] = {};
+static std::vector<std::pair<size_t, double*>> g_pinned_free;  // (doubles, buffer)
+constexpr size_t kPinnedKeep = 8;
+
+cudaMemPool_t oneshot_pool(const fkadj_options* opt) {
+    const char* v = getenv("FKADJ_ONESHOT_POOL");
+    if (v && v[0] == '0') return nullptr;
+    int dev = opt && opt->device >= 0 ? opt->device : -1;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_oneshot_mu);
+    if (!g_oneshot_pool[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;  // plain cudaMalloc then
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_oneshot_pool[dev] = pool;
+    }
+    return g_oneshot_pool[dev];
+}
+
+// A pinned buffer of at least n doubles (its capacity in *cap).
+static cudaError_t take_pinned(size_t n, double** p, size_t* cap) {
+    {
+        std::lock_guard<std::mutex> lk(g_oneshot_mu);
+        size_t best = g_pinned_free.size();
+        for (size_t i = 0; i < g_pinned_free.size(); ++i)
+            if (g_pinned_free[i].first >= n && (best == g_pinned_free.size() ||
+                                                g_pinned_free[i].first < g_pinned_free[best].first))
+                best = i;
+        if (best < g_pinned_free.size()) {
+            *cap = g_pinned_free[best].first;
+            *p = g_pinned_free[best].second;
+            g_pinned_free.erase(g_pinned_free.begin() + best);
+            return cudaSuccess;
+        }
+    }
+    *cap = n;
+    return cudaMallocHost(p, n * sizeof(double));
+}
+
+static void give_pinned(double* p, size_t cap) {
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_oneshot_mu);
+        if (g_pinned_free.size() < kPinnedKeep) {
+            g_pinned_free.emplace_back(cap, p);
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
+
+fkadj_status release_oneshot_memory() {
+    std::lock_guard<std::mutex> lk(g_oneshot_mu);
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) cur = 0;
+    cudaError_t e = cudaSuccess;
+    for (int dev = 0; dev < 64 && !e; ++dev) {
+        if (!g_oneshot_pool[dev]) continue;
+        // frees still in flight on other streams complete first
+        e = cudaSetDevice(dev);
+        if (!e) e = cudaDeviceSynchronize();
+        if (!e) e = cudaMemPoolTrimTo(g_oneshot_pool[dev], 0);
+    }
+    cudaSetDevice(cur);
+    for (auto& b : g_pinned_free) cudaFreeHost(b.second);
+    g_pinned_free.clear();
+    if (e) {
+        set_error(std::string("release cached memory: ") + cudaGetErrorString(e));
+        return FKADJ_ERR_CUDA;
+    }
+    return FKADJ_OK;
+}
+
 Problem::~Problem() {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     if (pool_) {
         // stream-ordered frees need the stream (the problem's own one is destroyed
         // below): release the buffers first
@@ -93,10 +188,32 @@ Problem::~Problem() {
     for (auto& e : ev_)
         if (e) cudaEventDestroy(e);
     drop_graph();
-    if (Ehost_) cudaFreeHost(Ehost_);
-    if (hres_) cudaFreeHost(hres_);
+    const auto t1 = clk::now();
+    if (oneshot_) {
+        give_pinned(Ehost_, Ehost_n_);
+        give_pinned(hres_, hres_n_);
+    } else {
+        if (Ehost_) cudaFreeHost(Ehost_);
+        if (hres_) cudaFreeHost(hres_);
+    }
+    const auto t2 = clk::now();
     if (own_stream_ && st_) cudaStreamDestroy(st_);
     delete spline_;
+    const auto t3 = clk::now();
+    if (verbose_ > 1) {
+        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &work_,
+                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
+                         &fcache_, &Ed_};
+        size_t bytes = 0;
+        for (DevBuf* b : all) bytes += b->bytes;
+        for (DevBuf* b : all) b->release();
+        const auto t4 = clk::now();
+        auto ms = [](clk::time_point a, clk::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        std::fprintf(stderr, "release: events %.1f ms, pinned %.1f ms, stream %.1f ms, device %.1f ms (%.2f GB)\n",
+                     ms(t0, t1), ms(t1, t2), ms(t2, t3), ms(t3, t4), bytes / 1e9);
+    }
 }
 
 bool Problem::GraphKey::operator==(const GraphKey& o) const {
@@ -165,6 +282,7 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     alpha_ = alpha;
     if (gamma) std::copy(gamma, gamma + 3, gamma_);
     grad_mode_ = o.grad_mode;
+    verbose_ = o.verbose;
     ckpt_policy_ = o.ckpt_policy;
     if (o.device >= 0) CK(cudaSetDevice(o.device), "cudaSetDevice");
     CK(cudaGetDevice(&device_), "cudaGetDevice");
@@ -341,7 +459,10 @@ fkadj_status Problem::prepare_E(const double* Et, bool upload) {
     const size_t n = (size_t)3 * nt_ + 1;
     if (!Ed_.p) {
         CK(Ed_.alloc(n * sizeof(double)), "alloc E tables");
-        CK(cudaMallocHost(&Ehost_, n * sizeof(double)), "alloc pinned E tables");
+        if (oneshot_)
+            CK(take_pinned(n, &Ehost_, &Ehost_n_), "alloc pinned E tables");
+        else
+            CK(cudaMallocHost(&Ehost_, n * sizeof(double)), "alloc pinned E tables");
         ++buf_gen_;
     } else {
         CK(cudaStreamSynchronize(st_), "synchronize");  // the previous upload is done with the staging
@@ -1105,10 +1226,16 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
     // per job)
     const size_t prow = (size_t)(3 * nt_ + 1);
     if (hres_n_ < prow + 1) {
-        if (hres_) cudaFreeHost(hres_);
-        hres_ = nullptr;
-        CK(cudaMallocHost(&hres_, (prow + 1) * sizeof(double)), "alloc pinned results");
-        hres_n_ = prow + 1;
+        if (oneshot_) {
+            give_pinned(hres_, hres_n_);
+            hres_ = nullptr;
+            CK(take_pinned(prow + 1, &hres_, &hres_n_), "alloc pinned results");
+        } else {
+            if (hres_) cudaFreeHost(hres_);
+            hres_ = nullptr;
+            CK(cudaMallocHost(&hres_, (prow + 1) * sizeof(double)), "alloc pinned results");
+            hres_n_ = prow + 1;
+        }
     }
     const int nt = nt_;
     CK(cudaEventRecord(ev_[0], st_), "event");
@@ -1238,6 +1365,7 @@ fkadj_status fkadj_forward(const fkadj_params* p, double dt, const double* Et, i
         return FKADJ_ERR_ARG;
     }
     Problem pb;
+    pb.set_oneshot(fkadj::oneshot_pool(opt));
     fkadj_status s = pb.init(*p, dt, nt, active_index, nrows, ncols, n_num, gh_num, nullptr, 0, nullptr, nullptr,
                              nullptr, 0.0, opt, false);
     if (s) return s;
@@ -1253,12 +1381,30 @@ fkadj_status fkadj_grad(const fkadj_params* p, double dt, const double* Et, int 
         fkadj::set_error("params is null");
         return FKADJ_ERR_ARG;
     }
-    Problem pb;
-    fkadj_status s = pb.init(*p, dt, nt, active_index, nrows, ncols, n_num, gh_num, gamma, S_ncol, S_colptr,
-                             S_rowidx, S_val, alpha, opt, true);
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    auto pb = std::make_unique<Problem>();
+    pb->set_oneshot(fkadj::oneshot_pool(opt));
+    fkadj_status s = pb->init(*p, dt, nt, active_index, nrows, ncols, n_num, gh_num, gamma, S_ncol, S_colptr,
+                              S_rowidx, S_val, alpha, opt, true);
     if (s) return s;
-    return pb.grad(Et, y_ini, L0, LE, Lcost, gradE, yf);
+    const auto t1 = clk::now();
+    s = pb->grad(Et, y_ini, L0, LE, Lcost, gradE, yf);
+    const auto t2 = clk::now();
+    const fkadj::Timing tm = pb->last_timing();
+    pb.reset();
+    const auto t3 = clk::now();
+    if (opt && opt->verbose > 0) {  // phase times of the one-shot call, to stderr
+        auto ms = [](clk::time_point a, clk::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        std::fprintf(stderr, "fkadj_grad: set-up %.1f ms, gradient %.1f ms (device: forward %.1f, backward %.1f), "
+                     "release %.1f ms\n", ms(t0, t1), ms(t1, t2), tm.fwd_ms, tm.bwd_ms, ms(t2, t3));
+    }
+    return s;
 }
+
+fkadj_status fkadj_release_cached_memory(void) { return fkadj::release_oneshot_memory(); }
 
 fkadj_status fkadj_problem_create(fkadj_problem** out, const fkadj_params* p, double dt, int nt,
                                   const int* active_index, int nrows, int ncols, int n_num, const double* gh_num,

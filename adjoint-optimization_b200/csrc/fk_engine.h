@@ -105,6 +105,12 @@ public:
     enum TileKind { T_FWD = 0, T_MID = 1, T_ADJ = 2, T_EXACT = 3 };
     // Stream-ordered device memory from `pool` (call before init).
     void use_pool(cudaMemPool_t pool) { pool_ = pool; }
+    // A problem of a one-shot entry point (call before init): device memory
+    // from `pool` (null: cudaMalloc), pinned staging from the process's cache.
+    void set_oneshot(cudaMemPool_t pool) {
+        pool_ = pool;
+        oneshot_ = true;
+    }
     int tile(int kind) const { return tk_[kind]; }
     void set_tile(int kind, int t) { tk_[kind] = t; }
     // rows per tile in use for a kernel kind (the preset's height, or fewer
@@ -188,6 +194,7 @@ private:
     bool autotune_ = true, tuned_ = false, tuned_fwd_ = false;
     bool own_stream_ = false, have_obj_ = false;
     cudaMemPool_t pool_ = nullptr;
+    int verbose_ = 0;
     int grad_mode_ = FKADJ_GRAD_REF, ckpt_policy_ = FKADJ_CKPT_AUTO;
     int64_t ckpt_budget_ = 0;
     cudaStream_t st_ = nullptr;
@@ -210,6 +217,8 @@ private:
     double* Ehost_ = nullptr;  // pinned staging of the E tables
     double* hres_ = nullptr;   // pinned results: L0 partial sum, then the z.gh rows
     size_t hres_n_ = 0;
+    size_t Ehost_n_ = 0;       // capacity of Ehost_ (doubles)
+    bool oneshot_ = false;
     bool have_y0_ = false;
 
     // captured gradient sequence
@@ -250,5 +259,10 @@ private:
     Timing timing_{};
     int64_t launches_ = 0;
 };
+
+// Memory the one-shot entry points keep between calls: the per-device pool
+// (null when FKADJ_ONESHOT_POOL=0) and its release (fkadj_release_cached_memory).
+cudaMemPool_t oneshot_pool(const fkadj_options* opt);
+fkadj_status release_oneshot_memory();
 
 }  // namespace fkadj

@@ -23,7 +23,8 @@ CKPT_AUTO, CKPT_FULL, CKPT_SQRT, CKPT_BINOMIAL = 0, 1, 2, 3
 # Every symbol include/fkadj.h declares (checked by the CPU tests).
 EXPORTS = (
     "fkadj_default_options", "fkadj_default_params", "fkadj_forward", "fkadj_grad",
-    "fkadj_param_string", "fkadj_last_error", "fkadj_problem_create", "fkadj_problem_destroy",
+    "fkadj_param_string", "fkadj_last_error", "fkadj_release_cached_memory", "fkadj_problem_create",
+    "fkadj_problem_destroy",
     "fkadj_problem_device_bytes", "fkadj_problem_objective", "fkadj_problem_grad",
     "fkadj_problem_last_timing", "fkadj_problem_last_launches", "fkadj_problem_set_profiling",
     "fkadj_problem_kernel_time", "fkadj_problem_tiles",
@@ -64,6 +65,8 @@ def load():
     L.fkadj_param_string.argtypes = [P]
     L.fkadj_param_string.restype = C.c_char_p
     L.fkadj_last_error.restype = C.c_char_p
+    L.fkadj_release_cached_memory.restype = C.c_int
+    L.fkadj_release_cached_memory.argtypes = []
     L.fkadj_problem_create.argtypes = [C.POINTER(C.c_void_p), P, C.c_double, C.c_int, ip, C.c_int,
                                        C.c_int, C.c_int, dp, dp, C.c_int64, i64p, i64p, dp, C.c_double, O]
     L.fkadj_problem_destroy.argtypes = [C.c_void_p]

@@ -88,6 +88,12 @@ def fk_forward_Et(Et, dt, nt, y0, active_index, ncols, nrows, ghost_lr, nstep, *
     return ys.T, yf, L.fkadj_param_string(C.byref(cp)).decode()
 
 
+def release_cached_memory():
+    """Hands back the device memory and pinned host staging that fk_forward_Et /
+    fk_grad_Et keep between calls (fkadj_release_cached_memory)."""
+    check(load().fkadj_release_cached_memory())
+
+
 def fk_grad_Et(Et, dt, nt, y0, active_index, ncols, nrows, ghost_lr, gamma, S, alpha, *,
                params: FkParams | None = None, opts=None, return_yf=False):
     """Returns (gradE[nt+1], Lcost, L0, LE, param_str) (+ yf when return_yf)."""

@@ -106,6 +106,15 @@ fkadj_status fkadj_grad(const fkadj_params *p, double dt, const double *Et, int 
                         const double *S_val, double alpha, double *L0, double *LE,
                         double *Lcost, double *gradE, double *yf, const fkadj_options *opt);
 
+/* fkadj_forward and fkadj_grad build their problem afresh on every call.  They
+ * keep its device memory (a stream-ordered pool per device) and its pinned
+ * host staging for the next call: freeing them at the end of each call, as
+ * the reference's MEX call does, was measured to stall a call by up to 0.8 s
+ * at times.  That memory stays with the process; this hands it back to the
+ * devices and the host (no counterpart in the reference).
+ * FKADJ_ONESHOT_POOL=0 in the environment allocates device memory per call. */
+fkadj_status fkadj_release_cached_memory(void);
+
 /* Parameter provenance text (the role of the reference's param_str).  The
  * returned string is owned by the library and valid until the next call from
  * the same thread. */
