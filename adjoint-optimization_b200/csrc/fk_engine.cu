@@ -190,6 +190,9 @@ Problem::~Problem() {
     drop_graph();
     const auto t1 = clk::now();
     if (oneshot_) {
+        // a failed call may leave copies to or from the staging in flight: let
+        // them finish before another call takes the buffers
+        if (st_ && (Ehost_ || hres_)) cudaStreamSynchronize(st_);
         give_pinned(Ehost_, Ehost_n_);
         give_pinned(hres_, hres_n_);
     } else {
