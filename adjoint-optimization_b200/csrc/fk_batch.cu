@@ -220,7 +220,7 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
     if ((s = P.prepare_E(Et, false))) return s;  // batched kernels take E by value
     j->Et.assign(Et, Et + P.nt_ + 1);
     if (want_grad) {
-        if ((s = P.plan_trajectory(j->tp))) return s;
+        if ((s = P.plan_trajectory(j->tp, true))) return s;
         if (j->tp.policy == FKADJ_CKPT_BINOMIAL) {
             set_error("batched jobs store full or sqrt trajectories; the binomial schedule runs in the "
                       "standalone engine (raise ckpt_budget_bytes or use fkadj_problem_grad)");
@@ -460,7 +460,10 @@ fkadj_status BatchEngine::finish_poll(Job& j) {
             for (int i = 0; i <= nt; ++i) j.gradE[i] = P.alpha_ * j.Et[i] - r[i];
         }
     }
-    j.status = std::isfinite(l0) ? FKADJ_OK : FKADJ_ERR_NUMERIC;
+    // the watchdog of the standalone gradient: objective and every gradient entry finite
+    bool finite = std::isfinite(l0);
+    for (size_t i = 0; finite && i < j.gradE.size(); ++i) finite = std::isfinite(j.gradE[i]);
+    j.status = finite ? FKADJ_OK : FKADJ_ERR_NUMERIC;
     j.done = true;
     j.t_done = host_seconds();
     return FKADJ_OK;

@@ -13,6 +13,8 @@
 //   bulk_arrive(bar, bytes);      __syncthreads();   // thread 0 posts the count
 //   bulk_issue<...>(bar, ...);    // one or more windows, bytes in total
 //   ok = bulk_wait(bar);          // false: the bounded wait expired
+// or, for one outcome across the CTA (and the fault word set on expiry),
+//   ok = bulk_wait_cta(bar, fault);
 #pragma once
 
 #include <cstdint>
@@ -67,23 +69,43 @@ __device__ __forceinline__ uint64_t bulk_now_ns() {
     return t;
 }
 
-// Waits for phase 0 of the barrier for at most about limit_ns of wall time
-// (and at most 2^22 polls); returns false when the wait expired.  Then the
-// posted bytes did not all arrive in time: the tile is incomplete, the caller
-// records the error and the host discards the call's results.
-__device__ __forceinline__ bool bulk_wait(uint32_t bar, uint64_t limit_ns = 1000000000ull) {
+// Waits for the phase of the barrier with the given parity (0 for its first
+// transfer, then 1, 0, ... when one barrier serves a sequence of transfers)
+// for at most about limit_ns of wall time (and at most 2^22 polls); returns
+// false when the wait expired.  Then the posted bytes did not all arrive in
+// time: the tile is incomplete, the caller records the error and the host
+// discards the call's results.
+__device__ __forceinline__ bool bulk_wait(uint32_t bar, uint64_t limit_ns = 1000000000ull, uint32_t parity = 0) {
     const uint64_t t0 = bulk_now_ns();
     for (int it = 0; it < (1 << 22); ++it) {
         uint32_t done;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
             : "=r"(done)
-            : "r"(bar)
+            : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
         if (bulk_now_ns() - t0 > limit_ns) break;
     }
     return false;
+}
+
+// bulk_wait for all threads of a CTA, with one outcome for all of them: true
+// when the posted bytes arrived.  When the wait expired in any thread, thread
+// 0 sets *fault (when non-null), the CTA waits once more, again bounded, for
+// copies still in flight, and every thread gets false: the window is
+// incomplete and the caller returns without computing or storing anything.
+// Copies that land after the second wait expired would write into shared
+// memory the CTA no longer owns; that is the risk this path leaves open.
+__device__ __forceinline__ bool bulk_wait_cta(uint32_t bar, unsigned* fault, uint64_t limit_ns = 1000000000ull,
+                                              uint32_t parity = 0) {
+    const bool ok = bulk_wait(bar, limit_ns, parity);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0 && fault) atomicOr(fault, 1u);
+        bulk_wait(bar, limit_ns, parity);
+        return false;
+    }
+    return true;
 }
 
 }  // namespace fkadj

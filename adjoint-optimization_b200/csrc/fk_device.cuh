@@ -24,6 +24,10 @@
 #ifndef FKADJ_OWN_RCP
 #define FKADJ_OWN_RCP 1
 #endif
+// 1/tau_v-(q) from q's exponential with one reciprocal (see tvm_rcp)
+#ifndef FKADJ_MERGED_TVM
+#define FKADJ_MERGED_TVM 1
+#endif
 
 namespace fkadj {
 
@@ -36,6 +40,7 @@ struct DevModel {
     double u_c, u_v, ksm, k_fk, u_csi;
     double r_tau_d, r_tau_0, r_tau_r, r_2tau_si;
     double tau_v1m, tau_v2m, r_tau_vp, r_tau_wm, r_tau_wp;
+    double r_tau_v2m;  // 1 / tau_v2_minus
     double dv12;  // tau_v2_minus - tau_v1_minus
     double eq;    // exp(-2 ksm (u_c - u_v)): e^{-2ksm(u-u_v)} = eq * e^{-2ksm(u-u_c)}
     double cu, cv, cw;  // D / h^2
@@ -101,24 +106,47 @@ __device__ __forceinline__ void steps_pq(const DevModel& P, double u, Step& sp, 
 #endif
 }
 
+// The voltage-dependent time scale tau_v-(q) = q tau_v1- + (1 - q) tau_v2- of
+// the v gate, with q = 1/(1 + eq), eq = e^{-2 ksm (u - u_v)}, only ever enters
+// as its reciprocal (and, in the Jacobian, through dq/du): since
+// tau_v- = (tau_v1- + eq tau_v2-) / (1 + eq),
+//   1/tau_v- = (1 + eq) rT   and   4 q (1 - q) / tau_v-^2 = 4 eq rT^2,
+// rT = 1 / (tau_v1- + eq tau_v2-): one reciprocal where q's logistic and the
+// time scale took two.  Same function, rounding moved by about an ulp.  For
+// eq beyond 1e300 (u < -3.4, far outside the model's range) the limits
+// 1/tau_v2- and 0 are taken.
+struct TvmRcp {
+    double r;    // 1 / tau_v-
+    double dqr;  // 4 q (1 - q) / tau_v-^2
+};
+__device__ __forceinline__ TvmRcp tvm_rcp(const DevModel& P, double eq) {
+    if (eq > 1e300) return {P.r_tau_v2m, 0.0};
+    const double rT = fk_rcp(fma(eq, P.tau_v2m, P.tau_v1m));
+    return {(1.0 + eq) * rT, (4.0 * eq) * (rT * rT)};
+}
+
 // Ionic currents (formula of cu-F:29-45): p, q and (1 + tanh)/2 of the slow
 // inward current are the three smoothed steps.
 __device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, double w,
                                        double& ud, double& vd, double& wd) {
+#if FKADJ_MERGED_TVM
+    const double e = exp(-2.0 * (P.ksm * (u - P.u_c)));
+    const Step sp = step_of_exp(e);
+    const double rtvm = tvm_rcp(P, e * P.eq).r;
+#else
     Step sp, sq;
     steps_pq(P, u, sp, sq);
+    const double q = sq.s;
+    const double tvm = q * P.tau_v1m + sq.c * P.tau_v2m;
+    const double rtvm = fk_rcp(tvm);
+#endif
     const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
-    const double p = sp.s, q = sq.s;
+    const double p = sp.s;
     const double j_fi = -v * p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
     const double j_so = u * sp.c * P.r_tau_0 + p * P.r_tau_r;
-    const double tvm = q * P.tau_v1m + sq.c * P.tau_v2m;
     const double j_si = -w * (2.0 * ss.s) * P.r_2tau_si;
     ud = -(j_fi + j_so + j_si);
-#if FKADJ_OWN_RCP
-    vd = (sp.c * (1.0 - v)) * own_rcp(tvm) - (p * v) * P.r_tau_vp;
-#else
-    vd = (sp.c * (1.0 - v)) / tvm - (p * v) * P.r_tau_vp;
-#endif
+    vd = (sp.c * (1.0 - v)) * rtvm - (p * v) * P.r_tau_vp;
     wd = (sp.c * (1.0 - w)) * P.r_tau_wm - (p * w) * P.r_tau_wp;
 }
 
@@ -131,15 +159,24 @@ struct JacT {
 
 // 1 - tanh^2 = 4 s (1 - s) for the smoothed step s.
 __device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, double w) {
+#if FKADJ_MERGED_TVM
+    const double e = exp(-2.0 * (P.ksm * (u - P.u_c)));
+    const Step sp = step_of_exp(e);
+    const TvmRcp tv = tvm_rcp(P, e * P.eq);
+    const double rtvm = tv.r, dq_rtvm2 = tv.dqr;
+#else
     Step sp, sq;
     steps_pq(P, u, sp, sq);
-    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
-    const double p = sp.s, q = sq.s;
-    const double dp = 4.0 * sp.s * sp.c;
+    const double q = sq.s;
     const double dq = 4.0 * sq.s * sq.c;
-    const double ds = 4.0 * ss.s * ss.c;
     const double tvm = q * P.tau_v1m + P.tau_v2m * sq.c;
     const double rtvm = fk_rcp(tvm);
+    const double dq_rtvm2 = dq * (rtvm * rtvm);
+#endif
+    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
+    const double p = sp.s;
+    const double dp = 4.0 * sp.s * sp.c;
+    const double ds = 4.0 * ss.s * ss.c;
     const double hk = 0.5 * dp * P.ksm;
     JacT J;
     J.a0 = -hk * P.r_tau_r + hk * v * (1.0 - u) * (u - P.u_c) * P.r_tau_d + hk * u * P.r_tau_0 +
@@ -147,8 +184,7 @@ __device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, d
            p * v * (u - P.u_c) * P.r_tau_d - sp.c * P.r_tau_0;
     J.a3 = p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
     J.a5 = (2.0 * ss.s) * P.r_2tau_si;
-    J.a1 = -hk * v * P.r_tau_vp - hk * (1.0 - v) * rtvm +
-           sp.c * (1.0 - v) * (0.5 * dq * P.ksm * P.dv12) * (rtvm * rtvm);
+    J.a1 = -hk * v * P.r_tau_vp - hk * (1.0 - v) * rtvm + sp.c * (1.0 - v) * (0.5 * P.ksm * P.dv12) * dq_rtvm2;
     J.a4 = -p * P.r_tau_vp - sp.c * rtvm;
     J.a2 = -hk * w * P.r_tau_wp - hk * (1.0 - w) * P.r_tau_wm;
     J.a6 = -p * P.r_tau_wp - sp.c * P.r_tau_wm;

@@ -43,6 +43,7 @@ static DevModel make_model(const fkadj_params& p, double dt) {
     M.r_2tau_si = 1.0 / (2 * p.tau_si);
     M.tau_v1m = p.tau_v1_minus;
     M.tau_v2m = p.tau_v2_minus;
+    M.r_tau_v2m = 1.0 / p.tau_v2_minus;
     M.r_tau_vp = 1.0 / p.tau_v_plus;
     M.r_tau_wm = 1.0 / p.tau_w_minus;
     M.r_tau_wp = 1.0 / p.tau_w_plus;
@@ -176,8 +177,8 @@ Problem::~Problem() {
     if (pool_) {
         // stream-ordered frees need the stream (the problem's own one is destroyed
         // below): release the buffers first
-        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &work_,
-                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
+        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
+                         &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
                          &fcache_, &Ed_};
         for (DevBuf* b : all) b->release();
     }
@@ -204,8 +205,8 @@ Problem::~Problem() {
     delete spline_;
     const auto t3 = clk::now();
     if (verbose_ > 1) {
-        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &work_,
-                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
+        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
+                         &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
                          &fcache_, &Ed_};
         size_t bytes = 0;
         for (DevBuf* b : all) bytes += b->bytes;
@@ -221,7 +222,7 @@ Problem::~Problem() {
 
 bool Problem::GraphKey::operator==(const GraphKey& o) const {
     if (policy != o.policy || nslots != o.nslots || seg_slots != o.seg_slots || keep_f != o.keep_f ||
-        exact != o.exact || gen != o.gen)
+        exact != o.exact || gen != o.gen || path != o.path || tkf != o.tkf)
         return false;
     for (int k = 0; k < 4; ++k)
         if (tk[k] != o.tk[k] || ty[k] != o.ty[k]) return false;
@@ -304,8 +305,8 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     }
     for (auto& e : ev_) CK(cudaEventCreate(&e), "cudaEventCreate");
     if (pool_) {
-        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &work_,
-                         &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
+        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
+                         &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
                          &fcache_, &Ed_};
         for (DevBuf* b : all) b->st = st_, b->pool = pool_;
     }
@@ -336,6 +337,23 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     autotune_ = o.tile <= 0 || o.tile > tile_count();
     for (int& t : tk_) t = autotune_ ? 0 : o.tile - 1;
     tuned_ = !autotune_;
+    // reference-mode backward step: split (k_adj_mid + k_adj_step) or fused
+    // (k_adj_fused, with the J_F(y)^T cache or re-evaluating it); the
+    // autotuner picks by time unless FKADJ_ADJ_PATH (split | fused |
+    // fused-recompute) fixes it, FKADJ_FUSED_TILE fixing the fused preset.
+    // A fixed tile preset (options.tile) keeps the split kernels.
+    forced_path_ = -1;
+    if (const char* ap = getenv("FKADJ_ADJ_PATH")) {
+        if (!std::strcmp(ap, "split")) forced_path_ = ADJ_SPLIT;
+        else if (!std::strcmp(ap, "fused")) forced_path_ = ADJ_FUSED;
+        else if (!std::strcmp(ap, "fused-recompute")) forced_path_ = ADJ_FUSED_RECOMPUTE;
+    }
+    tkf_ = 0;
+    if (const char* ft = getenv("FKADJ_FUSED_TILE")) {
+        const int t = std::atoi(ft);
+        if (t >= 0 && t < fused_count()) tkf_ = t;
+    }
+    adj_path_ = forced_path_ >= 0 ? forced_path_ : ADJ_SPLIT;
     subblock_lattice(g_, &nsbx_, &nsby_);
     nsb_ = nsbx_ * nsby_;
 
@@ -406,6 +424,8 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     CK(zc_.alloc((size_t)3 * n_num * sizeof(double)), "alloc compact");
     CK(opart_.alloc((size_t)objective_blocks(n_num) * sizeof(double)), "alloc partials");
     CK(osum_.alloc(sizeof(double)), "alloc sum");
+    CK(fault_.alloc(16), "alloc fault word");
+    CK(cudaMemsetAsync(fault_.p, 0, fault_.bytes, st_), "clear fault word");
     CK(work_.alloc(3 * state_bytes()), "alloc states");
     CK(cudaMemsetAsync(work_.p, 0xff, work_.bytes, st_), "init states");
     spline_ = new NakSpline(nt + 1, dt);
@@ -521,7 +541,7 @@ cudaError_t Problem::prof_end(int k) {
 
 fkadj_status Problem::check_fault() {
     unsigned f = 0;
-    CK(take_device_fault(st_, &f), "read the device fault flag");
+    CK(take_device_fault(st_, fault(), &f), "read the problem's fault word");
     if (f) {
         set_error("a bounded wait in a kernel expired (tile copy into shared memory); results are invalid");
         return FKADJ_ERR_TIMEOUT;
@@ -550,7 +570,8 @@ void Problem::kernel_time(int k, double* avg_ms, int64_t* samples) const {
 
 fkadj_status Problem::step_forward(int i, const double* yin, double* yout, double* k1) {
     CK(prof_begin(K_FWD), "profiling event");
-    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), efwd(i), st_, nullptr, ty_[T_FWD], k1),
+    CK(launch_fwd_step(tk_[T_FWD], P_, g_, yin, yout, gh_.as<double>(), efwd(i), st_, fault(), nullptr, ty_[T_FWD],
+                       k1),
        "forward step");
     CK(prof_end(K_FWD), "profiling event");
     ++launches_;
@@ -681,32 +702,53 @@ fkadj_status Problem::objective(const double* Et, const double* y_ini, double* L
     return FKADJ_OK;
 }
 
-fkadj_status Problem::plan_trajectory(TrajPlan& tp) {
+fkadj_status Problem::plan_trajectory(TrajPlan& tp, bool sqrt_or_full_only) {
     const double sb = (double)state_bytes();
     const int c = std::max(2, (int)std::ceil(std::sqrt((double)nt_)));
     const int sqrt_slots = (nt_ + c - 1) / c + 1 + (c - 1);
+    // binomial: y_0, y_nt and the free snapshots the budget holds, plus one scratch state
+    const int64_t bino_fit = (int64_t)((double)ckpt_budget_ / sb) - 1;
+    const int bino_slots = (int)std::max<int64_t>(2, std::min<int64_t>(bino_fit, nt_ + 1));
     int pol = ckpt_policy_;
     if (pol == FKADJ_CKPT_AUTO) {
-        if ((double)(nt_ + 1) * sb <= (double)ckpt_budget_) pol = FKADJ_CKPT_FULL;
-        else if ((double)sqrt_slots * sb <= (double)ckpt_budget_) pol = FKADJ_CKPT_SQRT;
-        else pol = FKADJ_CKPT_BINOMIAL;
+        if ((double)(nt_ + 1) * sb <= (double)ckpt_budget_) {
+            pol = FKADJ_CKPT_FULL;
+        } else if ((double)sqrt_slots * sb <= (double)ckpt_budget_) {
+            pol = FKADJ_CKPT_SQRT;
+            if (!sqrt_or_full_only && bino_fit >= 2) {
+                // recomputed forward steps: sqrt recomputes every segment but its
+                // first state; the binomial reversal what binomial_recompute_steps
+                // counts, plus (reference mode) about a third of a forward step per
+                // backward step for the work the sqrt store saves it (k1 kept
+                // beside the segment, no state copy per visit)
+                const int K = (nt_ + c - 1) / c;
+                const double sqrt_cost = (double)(nt_ - K);
+                const double bino_cost = (double)binomial_recompute_steps(nt_, bino_slots - 2) +
+                                         (grad_mode_ == FKADJ_GRAD_REF ? 0.35 * nt_ : 0.0);
+                if (bino_cost < sqrt_cost) pol = FKADJ_CKPT_BINOMIAL;
+            }
+        } else {
+            pol = FKADJ_CKPT_BINOMIAL;
+        }
     }
     tp.policy = pol;
     if (pol == FKADJ_CKPT_FULL) {
         tp.stride = 1;
         tp.nslots = nt_ + 1;
         tp.seg_slots = 0;
+        tp.recompute = 0;
     } else if (pol == FKADJ_CKPT_SQRT) {
         tp.stride = c;
         tp.nslots = (nt_ + c - 1) / c + 1;
         tp.seg_slots = c - 1;
+        tp.recompute = nt_ - (tp.nslots - 1);
     } else {
         // binomial: y_0, y_nt and s free snapshots within the budget, plus one
         // scratch state for replays when no snapshot is free
-        const int64_t fit = (int64_t)((double)ckpt_budget_ / sb) - 1;
         tp.stride = 0;
-        tp.nslots = (int)std::max<int64_t>(2, std::min<int64_t>(fit, nt_ + 1));
+        tp.nslots = bino_slots;
         tp.seg_slots = 1;
+        tp.recompute = binomial_recompute_steps(nt_, tp.nslots - 2);
     }
     const double need = (double)(tp.nslots + tp.seg_slots) * sb;
     if (ckpt_policy_ != FKADJ_CKPT_FULL && need > (double)ckpt_budget_) {
@@ -725,8 +767,10 @@ fkadj_status Problem::plan_trajectory(TrajPlan& tp) {
 
 fkadj_status Problem::ensure_traj(const TrajPlan& tp) {
     if (traj_.p && traj_plan_.policy == tp.policy && traj_plan_.nslots == tp.nslots &&
-        traj_plan_.seg_slots == tp.seg_slots && traj_plan_.keep_f == tp.keep_f)
+        traj_plan_.seg_slots == tp.seg_slots && traj_plan_.keep_f == tp.keep_f) {
+        traj_plan_ = tp;
         return FKADJ_OK;
+    }
     drop_graph();
     ++buf_gen_;
     traj_.release();
@@ -802,7 +846,8 @@ struct TuneKey {
 };
 struct TuneVal {
     int tk[4], ty[4];
-    bool adjoint;  // the adjoint kinds were tuned too
+    int tkf, path;  // fused preset and reference-adjoint path
+    bool adjoint;   // the adjoint kinds were tuned too
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
@@ -816,6 +861,7 @@ fkadj_status Problem::autotune() {
         auto it = g_tune.find(key);
         if (it != g_tune.end() && (it->second.adjoint || !want_adjoint)) {
             for (int k = 0; k < 4; ++k) tk_[k] = it->second.tk[k], ty_[k] = it->second.ty[k];
+            if (it->second.adjoint && forced_path_ < 0) tkf_ = it->second.tkf, adj_path_ = it->second.path;
             return FKADJ_OK;
         }
     }
@@ -824,6 +870,8 @@ fkadj_status Problem::autotune() {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         TuneVal v;
         for (int k = 0; k < 4; ++k) v.tk[k] = tk_[k], v.ty[k] = ty_[k];
+        v.tkf = tkf_;
+        v.path = adj_path_;
         v.adjoint = want_adjoint;
         g_tune[key] = v;
     }
@@ -858,8 +906,10 @@ fkadj_status Problem::autotune_trials() {
     };
     // every preset at its own height; the forward step and the midpoint also
     // with the rows that fit the grid into one wave of CTAs
+    float best_ms[4] = {0, 0, 0, 0};
     auto pick = [&](int kind, auto&& make_launch) -> cudaError_t {
-        float best = 1e30f;
+        float& best = best_ms[kind];
+        best = 1e30f;
         for (int t = 0; t < tile_count(); ++t) {
             int rows[2] = {0, 0}, nr = 1;  // 0 = the preset's height
             if (kind == T_FWD || kind == T_MID) {
@@ -877,7 +927,8 @@ fkadj_status Problem::autotune_trials() {
         return cudaSuccess;
     };
     cudaError_t e = pick(T_FWD, [&](int t, int ty) {
-        return launch_fwd_step(t, P_, g_, y, out, gh_.as<double>(), EStep::values(E, E, E), st_, nullptr, ty);
+        return launch_fwd_step(t, P_, g_, y, out, gh_.as<double>(), EStep::values(E, E, E), st_, fault(), nullptr,
+                               ty);
     });
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_REF) {
         double* z2 = zbuf_.as<double>() + state_elems();
@@ -887,24 +938,58 @@ fkadj_status Problem::autotune_trials() {
         // trial launches with the caches in use, as in the backward sweep
         e = pick(T_MID, [&](int t, int ty) {
             return launch_adj_mid(t, P_, g_, y, y, gh_.as<double>(), yh_.as<double>(), EStep::values(E, E, E), hw_,
-                                  st_, fc,
+                                  st_, fault(), fc,
                                   fc + 3 * pl, jc + 14 * pl, ty);
         });
         if (!e)
             e = pick(T_ADJ, [&](int t, int) {
                 return launch_adj_step(t, P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
-                                       partial_.as<double>(), nsbx_, st_, jc, jc + 14 * pl, jc + 7 * pl);
+                                       partial_.as<double>(), nsbx_, st_, fault(), jc, jc + 14 * pl, jc + 7 * pl);
             });
+        // the fused step against the split pair: every preset, with the J(y)
+        // cache and re-evaluating J(y); trial launches with kept f, as in the
+        // sqrt sweep
+        const float split_ms = best_ms[T_MID] + best_ms[T_ADJ];
+        float fused_best = 1e30f;
+        int fused_t = tkf_, fused_p = ADJ_FUSED;
+        const bool try_fused = forced_path_ != ADJ_SPLIT;
+        for (int t = 0; !e && try_fused && t < fused_count(); ++t) {
+            if (forced_path_ > 0 && getenv("FKADJ_FUSED_TILE") && t != tkf_) continue;
+            for (int path = ADJ_FUSED; !e && path <= ADJ_FUSED_RECOMPUTE; ++path) {
+                if (forced_path_ > 0 && path != forced_path_) continue;
+                const bool cache = path == ADJ_FUSED;
+                float ms = 0;
+                e = timed([&]() {
+                    return launch_adj_fused(t, P_, g_, y, z2, y, y, fc, fc + 3 * pl, nullptr, wc_.as<uint8_t>(),
+                                            gh_.as<double>(), EStep::values(E, E, E), hw_, partial_.as<double>(),
+                                            nsbx_, cache ? jc : nullptr, cache ? jc + 7 * pl : nullptr, st_, fault());
+                }, &ms);
+                launches_ += 10;
+                if (!e && ms < fused_best) fused_best = ms, fused_t = t, fused_p = path;
+            }
+        }
+        if (!e) {
+            if (forced_path_ >= 0) {
+                adj_path_ = forced_path_;
+                if (forced_path_ != ADJ_SPLIT) tkf_ = fused_t;
+            } else if (fused_best < split_ms) {
+                adj_path_ = fused_p;
+                tkf_ = fused_t;
+            } else {
+                adj_path_ = ADJ_SPLIT;
+            }
+        }
     }
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_EXACT) {
         double* z2 = zbuf_.as<double>() + state_elems();
-        e = launch_fwd_step(tk_[T_FWD], P_, g_, y, out, gh_.as<double>(), EStep::values(E, E, E), st_, stg_.as<double>(),
+        e = launch_fwd_step(tk_[T_FWD], P_, g_, y, out, gh_.as<double>(), EStep::values(E, E, E), st_, fault(),
+                            stg_.as<double>(),
                             ty_[T_FWD]);
         if (!e)
             e = pick(T_EXACT, [&](int t, int) {
                 double* p = partial_.as<double>();
                 return launch_adj_exact(t, P_, g_, y, z2, y, stg_.as<double>(), wc_.as<uint8_t>(),
-                                        gh_.as<double>(), p, p + nsb_, p + 2 * (size_t)nsb_, nsbx_, st_);
+                                        gh_.as<double>(), p, p + nsb_, p + 2 * (size_t)nsb_, nsbx_, st_, fault());
             });
     }
     // the trial launches wrote scratch partials: clear them
@@ -938,37 +1023,107 @@ fkadj_status Problem::advance(int a, int m, const double* src, double* dst) {
     return FKADJ_OK;
 }
 
-// Binomial (revolve) reversal of steps [a, b): visits j = b-1, ..., a in
-// that order, each with y_j, using the snapshot slots in `free` and
-// recomputing forward from y_a.  With s free slots and t = b - a steps, r is
-// the least number of sweeps with C(s + r, s) >= t (Griewank's binomial
-// bound); the checkpoint goes where the right part holds C(s - 1 + r, s - 1)
-// steps, which it can reverse with one slot fewer, and the left part holds at
-// most C(s + r - 1, s) steps, which it can reverse in one sweep fewer.
-fkadj_status Problem::reverse_binomial(int a, int b, double* ya, std::vector<double*>& free,
-                                       const std::function<fkadj_status(int, const double*)>& visit) {
-    fkadj_status s;
-    if (b - a == 1) return visit(a, ya);
-    const int ns = (int)free.size();
-    if (ns == 0) {  // no snapshot left: replay from y_a for every state
-        double* scr = segslot(0);
-        for (int j = b - 1; j > a; --j) {
-            if ((s = advance(a, j, ya, scr))) return s;
-            if ((s = visit(j, scr))) return s;
-        }
-        return visit(a, ya);
-    }
+// Where the binomial (revolve) schedule puts the checkpoint of a part [a, b)
+// with s >= 1 free slots: with t = b - a steps, r is the least number of sweeps
+// with C(s + r, s) >= t (Griewank's binomial bound); the checkpoint goes where
+// the right part holds C(s - 1 + r, s - 1) steps, which it can reverse with one
+// slot fewer, and the left part holds at most C(s + r - 1, s) steps, which it
+// can reverse in one sweep fewer.
+static int binomial_split(int a, int b, int s) {
     const int64_t t = b - a;
     int r = 1;
-    while (binom_small_k(ns + r, r) < t) ++r;
-    const int64_t right = std::min<int64_t>(binom_small_k(ns - 1 + r, r), t - 1);
-    const int m = b - (int)right;
-    double* sm = free.back();
-    free.pop_back();
-    if ((s = advance(a, m, ya, sm))) return s;
-    if ((s = reverse_binomial(m, b, sm, free, visit))) return s;
-    free.push_back(sm);
-    return reverse_binomial(a, m, ya, free, visit);
+    while (binom_small_k(s + r, r) < t) ++r;
+    const int64_t right = std::min<int64_t>(binom_small_k(s - 1 + r, r), t - 1);
+    return b - (int)right;
+}
+
+// The schedule's first chain of checkpoints: the split of [0, nt), then the
+// split of its right part, and so on while a part has more than one step and
+// a free slot.  These states lie on the forward sweep, which stores them as
+// it passes (each into the slot the reversal takes for it), so the reversal
+// does not recompute them.
+std::vector<int> binomial_spine(int nt, int free_slots) {
+    std::vector<int> spine;
+    int a = 0, s = free_slots;
+    while (nt - a > 1 && s > 0) {
+        a = binomial_split(a, nt, s--);
+        spine.push_back(a);
+    }
+    return spine;
+}
+
+// Forward steps the binomial reversal of nt steps recomputes with free_slots
+// free slots, the spine already stored by the forward sweep (the walk of
+// reverse_binomial without the launches).
+int64_t binomial_recompute_steps(int nt, int free_slots) {
+    struct Part { int a, b, s; bool spine; };
+    std::vector<Part> st{{0, nt, free_slots, true}};
+    int64_t steps = 0;
+    while (!st.empty()) {
+        const Part p = st.back();
+        st.pop_back();
+        const int64_t t = p.b - p.a;
+        if (t <= 1) continue;
+        if (p.s == 0) {
+            steps += t * (t - 1) / 2;
+            continue;
+        }
+        const int m = binomial_split(p.a, p.b, p.s);
+        if (!p.spine) steps += m - p.a;
+        st.push_back({p.a, m, p.s, false});
+        st.push_back({m, p.b, p.s - 1, p.spine});
+    }
+    return steps;
+}
+
+// Binomial (revolve) reversal of steps [0, nt): visits j = nt-1, ..., 0 in that
+// order, each with y_j, using the snapshot slots in `free` (the forward sweep
+// stored the spine's states in the slots this walk takes for them, so spine
+// parts are not advanced again) and recomputing forward from the nearest
+// checkpoint.  The walk of a part [a, b) with checkpoint m is: advance y_a to
+// y_m into a free slot, reverse [m, b), give the slot back, reverse [a, m).  It
+// runs from an explicit stack: with many slots the chain of right parts is as
+// long as the horizon.
+fkadj_status Problem::reverse_binomial(int nt, double* y0, std::vector<double*>& free,
+                                       const std::function<fkadj_status(int, const double*)>& visit) {
+    struct Task {
+        enum { REVERSE, RETURN_SLOT } kind;
+        int a, b;
+        double* ya;
+        bool spine;
+    };
+    std::vector<Task> st{{Task::REVERSE, 0, nt, y0, true}};
+    fkadj_status s;
+    while (!st.empty()) {
+        const Task k = st.back();
+        st.pop_back();
+        if (k.kind == Task::RETURN_SLOT) {
+            free.push_back(k.ya);
+            continue;
+        }
+        const int a = k.a, b = k.b;
+        if (b - a == 1) {
+            if ((s = visit(a, k.ya))) return s;
+            continue;
+        }
+        if (free.empty()) {  // no snapshot left: replay from y_a for every state
+            double* scr = segslot(0);
+            for (int j = b - 1; j > a; --j) {
+                if ((s = advance(a, j, k.ya, scr))) return s;
+                if ((s = visit(j, scr))) return s;
+            }
+            if ((s = visit(a, k.ya))) return s;
+            continue;
+        }
+        const int m = binomial_split(a, b, (int)free.size());
+        double* sm = free.back();
+        free.pop_back();
+        if (!k.spine && (s = advance(a, m, k.ya, sm))) return s;
+        st.push_back({Task::REVERSE, a, m, k.ya, false});
+        st.push_back({Task::RETURN_SLOT, 0, 0, sm, false});
+        st.push_back({Task::REVERSE, m, b, sm, k.spine});
+    }
+    return FKADJ_OK;
 }
 
 // Discrete-exact backward sweep: per step s (last to first) the forward step
@@ -981,12 +1136,12 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
     double* stg = stg_.as<double>();
     auto back = [&](int t, const double* y) -> fkadj_status {
         CK(prof_begin(K_FWD), "profiling event");
-        CK(launch_fwd_step(tk_[T_FWD], P_, g_, y, scratch, gh_.as<double>(), efwd(t), st_, stg, ty_[T_FWD]),
+        CK(launch_fwd_step(tk_[T_FWD], P_, g_, y, scratch, gh_.as<double>(), efwd(t), st_, fault(), stg, ty_[T_FWD]),
            "stage replay");
         CK(prof_end(K_FWD), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_exact(tk_[T_EXACT], P_, g_, lam, lam2, y, stg, wc_.as<uint8_t>(), gh_.as<double>(),
-                            prow(0, t), prow(1, t), prow(2, t), nsbx_, st_),
+                            prow(0, t), prow(1, t), prow(2, t), nsbx_, st_, fault()),
            "exact adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
@@ -1003,8 +1158,7 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
     if (tp.policy == FKADJ_CKPT_BINOMIAL) {
         std::vector<double*> free;
         for (int k = tp.nslots - 1; k >= 2; --k) free.push_back(slot(k));
-        return reverse_binomial(0, nt, slot(0), free,
-                                [&](int t, const double* y) { return back(t, y); });
+        return reverse_binomial(nt, slot(0), free, [&](int t, const double* y) { return back(t, y); });
     }
     for (int k = K - 1; k >= 0; --k) {
         const int s0 = k * c, s1 = std::min(s0 + c, nt);
@@ -1035,10 +1189,19 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
     };
     double* cur = slot(0);
     const bool binomial = tp.policy == FKADJ_CKPT_BINOMIAL;
+    // binomial: the forward sweep stores the schedule's spine; its k-th state
+    // goes to the k-th slot the reversal takes (free slots are taken from the
+    // back of nslots-1 .. 2)
+    const std::vector<int> spine = binomial ? binomial_spine(nt, tp.nslots - 2) : std::vector<int>();
+    size_t next_spine = 0;
     for (int i = 0; i < nt; ++i) {
         double* out;
         if (tp.policy == FKADJ_CKPT_FULL) out = slot(i + 1);
-        else if (binomial) out = (i + 1 == nt) ? slot(1) : ((cur == state_buf(1)) ? state_buf(2) : state_buf(1));
+        else if (binomial) {
+            if (i + 1 == nt) out = slot(1);
+            else if (next_spine < spine.size() && spine[next_spine] == i + 1) out = slot(2 + (int)next_spine++);
+            else out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
+        }
         else if ((i + 1) % c == 0) out = slot((i + 1) / c);
         else if (i + 1 == nt) out = slot(K);
         else out = (cur == state_buf(1)) ? state_buf(2) : state_buf(1);
@@ -1081,14 +1244,34 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
                          const double* fb) -> fkadj_status {
         const int nxt = 1 - cur_c;
         const double* fin = fb ? fb : (have_fcarry ? fc[cur_c] : nullptr);
+        if (adj_path_ != ADJ_SPLIT) {
+            // one launch: midpoint and the four stages (k_adj_fused); the
+            // J(y) cache of the previous step in the ADJ_FUSED path
+            const bool cache = adj_path_ == ADJ_FUSED;
+            CK(prof_begin(K_ADJ), "profiling event");
+            CK(launch_adj_fused(tkf_, P_, g_, z, z2, ya, yb, fa, fin, fa ? nullptr : fc[nxt], wc_.as<uint8_t>(),
+                                gh_.as<double>(), emid(i), hw_, prow(0, i - 1), nsbx_,
+                                (cache && have_jcarry) ? jy[cur_c] : nullptr, cache ? jy[nxt] : nullptr, st_,
+                                fault()),
+               "fused adjoint step");
+            CK(prof_end(K_ADJ), "profiling event");
+            launches_ += 1;
+            if ((i - 1) % pwin_ == 0) CK(flush_rows(0, i - 1, nt + 1), "reduce z.gh");
+            std::swap(z, z2);
+            cur_c = nxt;
+            have_fcarry = fa == nullptr;
+            have_jcarry = cache;
+            return FKADJ_OK;
+        }
         CK(prof_begin(K_MID), "profiling event");
-        CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), emid(i), hw_, st_, fin,
+        CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), emid(i), hw_, st_, fault(),
+                          fin,
                           fa ? nullptr : fc[nxt], jh, ty_[T_MID], fa),
            "adjoint midpoint");
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
-                           gh_.as<double>(), prow(0, i - 1), nsbx_, st_,
+                           gh_.as<double>(), prow(0, i - 1), nsbx_, st_, fault(),
                            have_jcarry ? jy[cur_c] : nullptr, jh, jy[nxt]),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
@@ -1116,7 +1299,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
             prev = keep;
             return FKADJ_OK;
         };
-        s = reverse_binomial(0, nt, slot(0), free, visit);
+        s = reverse_binomial(nt, slot(0), free, visit);
         if (s != FKADJ_OK) return s;
     } else if (tp.policy == FKADJ_CKPT_FULL) {
         // kept: f(y_t) for t < nt
@@ -1157,6 +1340,8 @@ Problem::GraphKey Problem::graph_key(const TrajPlan& tp, bool exact) const {
     key.keep_f = tp.keep_f;
     key.exact = exact;
     key.gen = buf_gen_;
+    key.path = adj_path_;
+    key.tkf = tkf_;
     for (int k = 0; k < 4; ++k) key.tk[k] = tk_[k], key.ty[k] = ty_[k];
     return key;
 }
@@ -1292,6 +1477,15 @@ fkadj_status Problem::grad(const double* Et, const double* y_ini, double* L0, do
         set_error("objective is not finite");
         return FKADJ_ERR_NUMERIC;
     }
+    // the adjoint sweep can overflow or turn NaN while y(T) and the objective
+    // stay finite; the reference has no such check (it exits only on CUDA
+    // errors, cu-G:1488-1496)
+    for (int i = 0; i <= nt; ++i)
+        if (!std::isfinite(gradE[i])) {
+            set_error("gradient is not finite at sample " + std::to_string(i) +
+                      " (the adjoint sweep overflowed or produced NaN); the objective is finite");
+            return FKADJ_ERR_NUMERIC;
+        }
     return FKADJ_OK;
 }
 
@@ -1457,6 +1651,31 @@ void fkadj_problem_last_timing(const fkadj_problem* pb, double out[3]) {
 }
 
 int64_t fkadj_problem_last_launches(const fkadj_problem* pb) { return pb ? pb->impl.last_launches() : 0; }
+
+void fkadj_problem_adjoint_kernel(const fkadj_problem* pb, int out[4]) {
+    if (!out) return;
+    out[0] = out[1] = out[2] = out[3] = 0;
+    if (!pb) return;
+    out[0] = pb->impl.adjoint_path();
+    if (out[0] != Problem::ADJ_SPLIT) {
+        const fkadj::TileShape t = fkadj::fused_shape(pb->impl.fused_tile());
+        out[1] = t.tx;
+        out[2] = t.ty;
+        out[3] = t.nt;
+    }
+}
+
+void fkadj_problem_last_plan(const fkadj_problem* pb, int64_t out[4]) {
+    if (!out) return;
+    out[0] = out[1] = out[2] = out[3] = 0;
+    if (!pb) return;
+    const fkadj::TrajPlan& tp = pb->impl.last_plan();
+    if (!pb->impl.has_trajectory()) return;
+    out[0] = tp.policy;
+    out[1] = tp.nslots;
+    out[2] = tp.seg_slots;
+    out[3] = tp.recompute;
+}
 
 void fkadj_problem_tiles(const fkadj_problem* pb, int out[4], int shapes[12]) {
     if (!pb || !out) return;

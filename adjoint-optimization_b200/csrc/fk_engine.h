@@ -63,6 +63,7 @@ struct TrajPlan {
     int seg_slots = 0;             // recompute buffer slots
     bool keep_f = false;           // k1 = f(y_t, Et[t]) kept beside the states the
                                    // backward sweep walks (FULL: all, SQRT: the segment)
+    int64_t recompute = 0;         // forward steps the backward sweep recomputes
 };
 
 class BatchEngine;
@@ -90,6 +91,9 @@ public:
     static int64_t estimate_bytes(int nrows, int ncols, int nt, int n_num, int64_t nnz, int grad_mode,
                                   int policy, bool want_grad);
     Timing last_timing() const { return timing_; }
+    // trajectory plan of the last gradient (policy FULL/SQRT/BINOMIAL, 0 = none yet)
+    const TrajPlan& last_plan() const { return traj_plan_; }
+    bool has_trajectory() const { return traj_.p != nullptr; }
     int64_t last_launches() const { return launches_; }
 
     // Sampled per-kernel device times (CUDA events around every k-th launch
@@ -103,6 +107,11 @@ public:
     cudaStream_t stream() const { return st_; }
     // tile preset per kernel kind; chosen by autotune() unless fixed by options
     enum TileKind { T_FWD = 0, T_MID = 1, T_ADJ = 2, T_EXACT = 3 };
+    // reference-mode backward step: k_adj_mid + k_adj_step, or k_adj_fused
+    // reading the cached J_F(y_i)^T, or k_adj_fused evaluating it
+    enum AdjPath { ADJ_SPLIT = 0, ADJ_FUSED = 1, ADJ_FUSED_RECOMPUTE = 2 };
+    int adjoint_path() const { return adj_path_; }
+    int fused_tile() const { return tkf_; }
     // Stream-ordered device memory from `pool` (call before init).
     void use_pool(cudaMemPool_t pool) { pool_ = pool; }
     // A problem of a one-shot entry point (call before init): device memory
@@ -142,13 +151,19 @@ private:
     fkadj_status prof_collect();
     // FKADJ_ERR_TIMEOUT when a kernel's bounded wait expired since the last check
     fkadj_status check_fault();
-    fkadj_status plan_trajectory(TrajPlan& tp);
+    // Resolves the checkpoint policy.  AUTO takes FULL when the budget holds
+    // every state, else whichever of SQRT and BINOMIAL fits and recomputes
+    // fewer forward steps (costed in forward-step equivalents, the binomial
+    // reference-mode reversal's extra per-step work included); with
+    // sqrt_or_full_only (the batch engine, which runs no binomial schedule)
+    // BINOMIAL only when SQRT does not fit.
+    fkadj_status plan_trajectory(TrajPlan& tp, bool sqrt_or_full_only = false);
     fkadj_status ensure_traj(const TrajPlan& tp);
     fkadj_status run_objective(const double* yT, double* L0);
     fkadj_status objective_async(const double* yT);
     fkadj_status grad_exact_backward(const TrajPlan& tp, double* lam, double* lam2);
     fkadj_status advance(int a, int m, const double* src, double* dst);
-    fkadj_status reverse_binomial(int a, int b, double* ya, std::vector<double*>& free,
+    fkadj_status reverse_binomial(int nt, double* y0, std::vector<double*>& free,
                                   const std::function<fkadj_status(int, const double*)>& visit);
     // all_rows: keep the z.gh partials of every step (the batch engine);
     // otherwise a window of kPartialWindow rows reduced as the sweep goes.
@@ -190,6 +205,9 @@ private:
     double dt_ = 0, alpha_ = 0, gamma_[3] = {0, 0, 0};
     int nt_ = 0, n_num_ = 0, device_ = 0, nsbx_ = 0, nsby_ = 0, nsb_ = 0;
     int tk_[4] = {0, 0, 0, 0};  // tile preset per kernel kind (TileKind)
+    int tkf_ = 0;               // fused reference-adjoint preset (fused_shape)
+    int adj_path_ = 0;          // AdjPath of the reference-mode backward step
+    int forced_path_ = -1;      // AdjPath fixed by FKADJ_ADJ_PATH (-1: autotuned)
     int ty_[4] = {0, 0, 0, 0};  // rows per tile per kind (0 = the preset's height)
     bool autotune_ = true, tuned_ = false, tuned_fwd_ = false;
     bool own_stream_ = false, have_obj_ = false;
@@ -202,6 +220,8 @@ private:
 
     // device buffers
     DevBuf gh_, wc_, pos_, Srow_, Scol_, Sval_, yc_, zc_, opart_, osum_;
+    DevBuf fault_;     // this problem's fault word: set by a step kernel whose bounded wait expired
+    unsigned* fault() const { return fault_.as<unsigned>(); }
     DevBuf work_;      // 4 states: two ping-pong, z pair is separate
     DevBuf zbuf_;      // 2 adjoint states
     DevBuf yh_;        // midpoint state
@@ -223,7 +243,7 @@ private:
 
     // captured gradient sequence
     struct GraphKey {
-        int policy = -1, nslots = 0, seg_slots = 0, keep_f = 0, exact = 0, gen = 0;
+        int policy = -1, nslots = 0, seg_slots = 0, keep_f = 0, exact = 0, gen = 0, path = 0, tkf = 0;
         int tk[4] = {0, 0, 0, 0}, ty[4] = {0, 0, 0, 0};
         bool operator==(const GraphKey& o) const;
     };
@@ -259,6 +279,11 @@ private:
     Timing timing_{};
     int64_t launches_ = 0;
 };
+
+// The binomial schedule's first chain of checkpoints (the states the forward
+// sweep stores), and the forward steps its reversal then recomputes.
+std::vector<int> binomial_spine(int nt, int free_slots);
+int64_t binomial_recompute_steps(int nt, int free_slots);
 
 // Memory the one-shot entry points keep between calls: the per-device pool
 // (null when FKADJ_ONESHOT_POOL=0) and its release (fkadj_release_cached_memory).

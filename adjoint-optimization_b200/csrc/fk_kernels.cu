@@ -111,10 +111,6 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
     }
 }
 
-// Set when a bounded wait in a kernel gave up (read and cleared by the host
-// after each call: take_device_fault).
-__device__ unsigned int g_device_fault = 0;
-
 // Tile loads through the bulk-copy engine (fk_bulk.cuh) in the one-tile-per-CTA
 // step kernels; FKADJ_BULK_LOAD=0 keeps the vector loads everywhere.
 #ifndef FKADJ_BULK_LOAD
@@ -124,27 +120,52 @@ __device__ unsigned int g_device_fault = 0;
 // Copies one window (d1 null) or two windows of the same shape into shared
 // memory: through the bulk-copy engine when BULK and the windows start on an
 // even column, else with vector loads.  Ends with the CTA synchronised.
+// Returns false when the bounded wait for the bulk copies expired in any
+// thread of the CTA (bulk_wait_cta): the tile is then incomplete, *fault (the
+// problem's own fault word, read and cleared by the host after each call) is
+// set, and the caller returns without computing or storing anything.
+// A third window (d2, s2) may follow the first two.  A CTA that loads several
+// tiles in turn (the batched kernels) passes `phase`, its count of bulk
+// transfers so far, the same in every thread: the barrier is initialised at
+// the first transfer only and each later one waits on the next phase's
+// parity (a barrier is not re-initialised while in use).
 template <int RCAP, int WIDTH, int NT, bool BULK>
-__device__ __forceinline__ void load_windows(double* __restrict__ d0, const double* __restrict__ s0,
+__device__ __forceinline__ bool load_windows(double* __restrict__ d0, const double* __restrict__ s0,
                                              double* __restrict__ d1, const double* __restrict__ s1, int ld,
-                                             long long plane, bool vec_ok, int rows) {
+                                             long long plane, bool vec_ok, int rows, unsigned* fault,
+                                             double* __restrict__ d2 = nullptr,
+                                             const double* __restrict__ s2 = nullptr, uint32_t* phase = nullptr) {
     // every row start 16-byte aligned, checked on the addresses themselves
     const bool aligned = vec_ok && ((reinterpret_cast<uintptr_t>(s0) | reinterpret_cast<uintptr_t>(s1) |
-                                     (uintptr_t)ld * 8u | (uintptr_t)plane * 8u) & 15) == 0;
+                                     reinterpret_cast<uintptr_t>(s2) | (uintptr_t)ld * 8u | (uintptr_t)plane * 8u) &
+                                    15) == 0;
     if (BULK && FKADJ_BULK_LOAD && aligned) {
         __shared__ uint64_t bar;
-        const uint32_t b = bulk_begin(&bar);
+        const uint32_t k = phase ? *phase : 0u;
+        uint32_t b;
+        if (k == 0) {
+            b = bulk_begin(&bar);
+        } else {
+            b = (uint32_t)__cvta_generic_to_shared(&bar);
+            // the CTA's earlier reads and writes of these buffers (previous
+            // tile) before the copies' writes through the async proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
         __syncthreads();
-        bulk_arrive(b, bulk_bytes<WIDTH>(rows) * (d1 ? 2u : 1u));
+        bulk_arrive(b, bulk_bytes<WIDTH>(rows) * (1u + (d1 ? 1u : 0u) + (d2 ? 1u : 0u)));
         __syncthreads();
         bulk_issue<RCAP, WIDTH, NT>(b, d0, s0, ld, plane, rows);
         if (d1) bulk_issue<RCAP, WIDTH, NT>(b, d1, s1, ld, plane, rows);
-        if (!bulk_wait(b)) atomicOr(&g_device_fault, 1u);
+        if (d2) bulk_issue<RCAP, WIDTH, NT>(b, d2, s2, ld, plane, rows);
+        if (phase) ++*phase;
+        if (!bulk_wait_cta(b, fault, 1000000000ull, k & 1u)) return false;
     } else {
         load_region<RCAP, WIDTH, NT>(d0, s0, ld, plane, vec_ok, rows);
         if (d1) load_region<RCAP, WIDTH, NT>(d1, s1, ld, plane, vec_ok, rows);
+        if (d2) load_region<RCAP, WIDTH, NT>(d2, s2, ld, plane, vec_ok, rows);
     }
     __syncthreads();
+    return true;
 }
 
 // Fixed-order block sum (warp shuffles, then warps in order); result valid in
@@ -271,7 +292,8 @@ template <int TX, int TY, int NT, bool BULK = false>
 __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ yin,
                                               double* __restrict__ yout, const double* __restrict__ gh, double E0,
                                               double Eh, double E1, double* __restrict__ stages, int tbx, int tby,
-                                              int ty, double* __restrict__ k1 = nullptr) {
+                                              int ty, double* __restrict__ k1 = nullptr,
+                                              unsigned* fault = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -282,7 +304,9 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     // region origin: logical (i0 - HALO, j0 - HALO) = padded (i0, j0)
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_windows<RH, RW, NT, BULK>(A, yin + off, nullptr, nullptr, g.ld, g.plane, vec_ok, rows + 2 * HALO);
+    if (!load_windows<RH, RW, NT, BULK>(A, yin + off, nullptr, nullptr, g.ld, g.plane, vec_ok, rows + 2 * HALO,
+                                        fault))
+        return;
     const double* y0g = yin + off;
     const double* ghs = gh + off;
     const double dt = P.dt;
@@ -304,9 +328,10 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_fwd_step(DevModel P, DevGrid g, const double* __restrict__ yin, double* __restrict__ yout,
                const double* __restrict__ gh, EStep E, double* __restrict__ stages, int ty,
-               double* __restrict__ k1) {
+               double* __restrict__ k1, unsigned* fault) {
     pdl_enter();
-    fwd_step_tile<TX, TY, NT, true>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1);
+    fwd_step_tile<TX, TY, NT, true>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1,
+                                    fault);
 }
 
 // ------------------------------------------------- reference-mode adjoint
@@ -349,7 +374,8 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
                                              double* __restrict__ yh, double Ea, double Eb, double E3,
                                              const HermiteW& hw, const double* __restrict__ fin,
                                              double* __restrict__ fout, double* __restrict__ jh, int tbx, int tby,
-                                             int ty, const double* __restrict__ fa = nullptr) {
+                                             int ty, const double* __restrict__ fa = nullptr,
+                                             unsigned* fault = nullptr) {
     constexpr int H2 = 2;
     constexpr int RW = TX + 2 * H2, RH = TY + 2 * H2, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
@@ -362,7 +388,8 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
     // region origin: logical (i0 - 2, j0 - 2) = padded (i0 + 2, j0 + 2)
     const long long off = (long long)(i0 + HALO - H2) * g.ld + (j0 + HALO - H2);
     const bool vec_ok = ((g.ld | (j0 + HALO - H2)) & 1) == 0;
-    load_windows<RH, RW, NT, BULK>(A, ya + off, B, yb + off, g.ld, g.plane, vec_ok, rows + 2 * H2);
+    if (!load_windows<RH, RW, NT, BULK>(A, ya + off, B, yb + off, g.ld, g.plane, vec_ok, rows + 2 * H2, fault))
+        return;
     const double dt = P.dt;
     {
         constexpr int W = TX + 2;
@@ -435,10 +462,10 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_adj_mid(DevModel P, DevGrid g, const double* __restrict__ ya, const double* __restrict__ yb,
               const double* __restrict__ gh, double* __restrict__ yh, EStep E, HermiteW hw,
               const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty,
-              const double* __restrict__ fa) {
+              const double* __restrict__ fa, unsigned* fault) {
     pdl_enter();
     adj_mid_tile<TX, TY, NT, true>(P, g, ya, yb, gh, yh, E.a(), E.b(), E.c(), hw, fin, fout, jh, blockIdx.x, blockIdx.y,
-                             ty, fa);
+                                   ty, fa, fault);
 }
 
 // One adjoint stage on the tile grown by E cells: k = L^T src + J_F(y)^T src,
@@ -532,7 +559,7 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
                                               const uint8_t* __restrict__ wc, const double* __restrict__ gh,
                                               double* __restrict__ row, int nsbx, const double* __restrict__ jb,
                                               const double* __restrict__ jh, double* __restrict__ ja, int tbx,
-                                              int tby) {
+                                              int tby, unsigned* fault = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -541,7 +568,7 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_windows<RH, RW, NT, BULK>(A, z + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH);
+    if (!load_windows<RH, RW, NT, BULK>(A, z + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH, fault)) return;
     const double dt = P.dt;
     adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb, nullptr);
     adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
@@ -556,9 +583,209 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_adj_step(DevModel P, DevGrid g, const double* __restrict__ z, double* __restrict__ zout,
                const double* __restrict__ yb, const double* __restrict__ yh, const double* __restrict__ ya,
                const uint8_t* __restrict__ wc, const double* __restrict__ gh, double* __restrict__ row, int nsbx,
-               const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja) {
+               const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja,
+               unsigned* fault) {
     pdl_enter();
-    adj_step_tile<TX, TY, NT, true>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y);
+    adj_step_tile<TX, TY, NT, true>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y,
+                                    fault);
+}
+
+// ------------------------------------------- fused reference-mode adjoint
+//
+// One backward step of the reference adjoint in one launch: the midpoint
+// reconstruction of k_adj_mid and the four stages of k_adj_step, with the
+// midpoint state and its Jacobian never leaving the CTA.  The tile's windows
+// of z, y_{i-1} and y_i (tile + 4) arrive by bulk copies; y(1/3) is formed on
+// the tile + 3 and f(y(1/3)) on the tile + 2, so yh covers the region stage 2
+// reads; J_F(yh)^T is evaluated where stages 2 and 3 need it instead of being
+// stored and reloaded (k_adj_mid writes 80 B/cell that k_adj_step reads about
+// 2.3 times).  Every value is the same computation on the same inputs as in
+// the split kernels (cu-G:1244-1301 then cu-G:1349-1427 in the order of
+// cu-G:1885-1891), so the gradient does not depend on which path runs.
+//
+// Stage 1's J_F(y_i)^T comes from the cache jb left by the previous step's
+// stage 4 (which stores J_F(y_{i-1})^T to ja), or, with jb null, is evaluated
+// from the y_i window; with ja null nothing is stored.  fa / fb are f(y_{i-1})
+// and f(y_i) where kept or carried (null: evaluated from the windows); fout
+// receives the evaluated f(y_{i-1}) on the tile for the next step's fb.
+//
+// One stage on the tile grown by E cells, k_adj_step's algebra with the
+// step-start state z0 read from its shared-memory window Zw; jac(r, c, o)
+// returns J_F^T at window cell (r, c), global offset o (called for non-hole
+// cells only).
+template <int E, int TX, int TY, int NT, int MODE, class Jac>
+__device__ __forceinline__ void fused_stage(const DevModel& P, const DevGrid& g, const double* __restrict__ src,
+                                            double* __restrict__ dst, double* __restrict__ D,
+                                            const double* __restrict__ Zw, const uint8_t* __restrict__ wc,
+                                            long long off, double cZ, double cD, double* __restrict__ out,
+                                            const double* __restrict__ gh, Jac jac) {
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
+    constexpr int IN = TX * TY;
+    RowCol<W, NT> rc(HALO - E, HALO - E);
+#pragma unroll kStageUnroll
+    for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
+        const int r = rc.r, c = rc.c;
+        const int s = r * RW + c;
+        const long long o = off + (long long)r * g.ld + c;
+        const double a = Zw[s], b = Zw[RN + s], e = Zw[2 * RN + s];
+        const int code = __ldg(wc + o);
+        double ku, kv, kw;
+#if FKADJ_HOLE_BRANCH
+        if (isnan(src[s])) {  // holes and the NaN ring: the result is NaN
+            ku = kv = kw = src[s];
+        } else
+#endif
+        {
+            const JacT J = jac(r, c, o);
+            adj_at<RW, RN>(P, src, s, code, J, ku, kv, kw);
+        }
+        const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+        const int d = (r - HALO) * TX + (c - HALO);
+        if (MODE == 2) {
+            const double nu = (a + D[d]) + cD * ku;
+            out[o] = nu;
+            out[g.plane + o] = (b + D[IN + d]) + cD * kv;
+            out[2 * g.plane + o] = (e + D[2 * IN + d]) + cD * kw;
+            const double t = nu * __ldg(gh + o);
+            D[d] = isnan(t) ? 0.0 : t;
+        } else {
+            dst[s] = a + cZ * ku;
+            dst[RN + s] = b + cZ * kv;
+            dst[2 * RN + s] = e + cZ * kw;
+            if (inner) {
+                if (MODE == 0) {
+                    D[d] = cD * ku;
+                    D[IN + d] = cD * kv;
+                    D[2 * IN + d] = cD * kw;
+                } else {
+                    D[d] = D[d] + cD * ku;
+                    D[IN + d] = D[IN + d] + cD * kv;
+                    D[2 * IN + d] = D[2 * IN + d] + cD * kw;
+                }
+            }
+        }
+    }
+    if (MODE != 2) __syncthreads();
+}
+
+// Shared memory of k_adj_fused: windows of z, y_{i-1}, y_i on the tile + 4,
+// y(1/3) on the tile + 3, the quartic part of yh (then yh) on the tile + 2,
+// and the stage accumulator (206 KB at 32x32, 219 KB at 64x16).
+template <int TX, int TY>
+constexpr size_t fused_smem_bytes() {
+    return sizeof(double) * (9 * (TX + 2 * HALO) * (TY + 2 * HALO) + 3 * (TX + 6) * (TY + 6) +
+                             3 * (TX + 4) * (TY + 4) + 3 * TX * TY);
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    k_adj_fused(DevModel P, DevGrid g, const double* __restrict__ z, double* __restrict__ zout,
+                const double* __restrict__ ya, const double* __restrict__ yb, const double* __restrict__ fa,
+                const double* __restrict__ fb, double* __restrict__ fout, const uint8_t* __restrict__ wc,
+                const double* __restrict__ gh, EStep E, HermiteW hw, double* __restrict__ row, int nsbx,
+                const double* __restrict__ jb, double* __restrict__ ja, unsigned* fault) {
+    pdl_enter();
+    constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;  // windows: tile + 4
+    constexpr int W3 = TX + 6, RN3 = W3 * (TY + 6);                      // y(1/3): tile + 3
+    constexpr int WQ = TX + 4, RNQ = WQ * (TY + 4);                      // quartic part / yh: tile + 2
+    extern __shared__ double4 smem_raw[];
+    double* Zw = reinterpret_cast<double*>(smem_raw);
+    double* YA = Zw + 3 * RN;  // y_{i-1}; stage 2 writes its state here
+    double* YB = YA + 3 * RN;  // y_i; stages 1 and 3 write their states here
+    double* Y3 = YB + 3 * RN;
+    double* Q = Y3 + 3 * RN3;
+    double* D = Q + 3 * RNQ;
+    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const long long off = (long long)i0 * g.ld + j0;  // window origin: logical (i0 - 4, j0 - 4)
+    const bool vec_ok = ((g.ld | j0) & 1) == 0;
+    if (!load_windows<RH, RW, NT, true>(Zw, z + off, YA, ya + off, g.ld, g.plane, vec_ok, RH, fault, YB, yb + off))
+        return;
+    const double dt = P.dt;
+    const double Ea = E.a(), Eb = E.b(), E3 = E.c();
+    // y(1/3) (cubic Hermite) on the tile + 3 and the quartic part of yh on the tile + 2
+    {
+        constexpr int W = TX + 6;
+        constexpr int N = W * (TY + 6);
+        RowCol<W, NT> rc(1, 1);
+#pragma unroll kStageUnroll
+        for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
+            const int r = rc.r, c = rc.c;
+            const int s = r * RW + c;
+            const long long o = off + (long long)r * g.ld + c;
+            const double gg = __ldg(gh + o);
+            double a0[3], a1[3];
+            if (fa) {
+                a0[0] = __ldg(fa + o);
+                a0[1] = __ldg(fa + g.plane + o);
+                a0[2] = __ldg(fa + 2 * g.plane + o);
+            } else {
+                rhs_at<RW, RN>(P, YA, s, Ea * gg, a0[0], a0[1], a0[2]);
+            }
+            if (fb) {
+                a1[0] = __ldg(fb + o);
+                a1[1] = __ldg(fb + g.plane + o);
+                a1[2] = __ldg(fb + 2 * g.plane + o);
+            } else {
+                rhs_at<RW, RN>(P, YB, s, Eb * gg, a1[0], a1[1], a1[2]);
+            }
+            if (fout && r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX) {
+                fout[o] = a0[0];
+                fout[g.plane + o] = a0[1];
+                fout[2 * g.plane + o] = a0[2];
+            }
+            const int s3 = (r - 1) * W3 + (c - 1);
+            const bool qcell = r >= 2 && r < RH - 2 && c >= 2 && c < RW - 2;
+            const int sq = (r - 2) * WQ + (c - 2);
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                const double m0 = a0[f] * dt, m1 = a1[f] * dt;
+                const double x0 = YA[f * RN + s], x1 = YB[f * RN + s];
+                Y3[f * RN3 + s3] = ((hw.c3[0] * x0 + hw.c3[1] * m0) + hw.c3[2] * x1) + hw.c3[3] * m1;
+                if (qcell) Q[f * RNQ + sq] = ((hw.c4[0] * x0 + hw.c4[1] * m0) + hw.c4[2] * x1) + hw.c4[3] * m1;
+            }
+        }
+    }
+    __syncthreads();
+    // yh = quartic part + (27/64) dt f(y(1/3), E(t_{i-1} + dt/3)) on the tile + 2
+    {
+        constexpr int W = TX + 4;
+        constexpr int N = W * (TY + 4);
+        RowCol<W, NT> rc(2, 2);
+#pragma unroll kStageUnroll
+        for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
+            const int r = rc.r, c = rc.c;
+            const long long o = off + (long long)r * g.ld + c;
+            const int s3 = (r - 1) * W3 + (c - 1);
+            const int sq = (r - 2) * WQ + (c - 2);
+            double m2[3];
+            rhs_at<W3, RN3>(P, Y3, s3, E3 * __ldg(gh + o), m2[0], m2[1], m2[2]);
+#pragma unroll
+            for (int f = 0; f < 3; ++f) Q[f * RNQ + sq] = Q[f * RNQ + sq] + hw.c2 * (m2[f] * dt);
+        }
+    }
+    __syncthreads();
+    // the four backward stages (k_adj_step's): J(y_i), J(yh), J(yh), J(y_{i-1})
+    auto j_yb = [&](int r, int c, long long o) -> JacT {
+        if (jb) return load_jac(jb, g.plane, o);
+        const int s = r * RW + c;
+        return fk_jacT(P, finite_u(YB[s]), YB[RN + s], YB[2 * RN + s]);
+    };
+    auto j_yh = [&](int r, int c, long long) -> JacT {
+        const int sq = (r - 2) * WQ + (c - 2);
+        return fk_jacT(P, Q[sq], Q[RNQ + sq], Q[2 * RNQ + sq]);
+    };
+    auto j_ya = [&](int, int, long long o) -> JacT {
+        const JacT J = fk_jacT(P, finite_u(__ldg(ya + o)), __ldg(ya + g.plane + o), __ldg(ya + 2 * g.plane + o));
+        if (ja) store_jac(ja, g.plane, o, J);
+        return J;
+    };
+    fused_stage<3, TX, TY, NT, 0>(P, g, Zw, YB, D, Zw, wc, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, j_yb);
+    fused_stage<2, TX, TY, NT, 1>(P, g, YB, YA, D, Zw, wc, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, j_yh);
+    fused_stage<1, TX, TY, NT, 1>(P, g, YA, YB, D, Zw, wc, off, dt, 2.0 / 6.0 * dt, nullptr, gh, j_yh);
+    fused_stage<0, TX, TY, NT, 2>(P, g, YB, YA, D, Zw, wc, off, 0.0, 1.0 / 6.0 * dt, zout, gh, j_ya);
+    __syncthreads();
+    subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
 }
 
 // ------------------------------------------------------ exact-mode adjoint
@@ -637,7 +864,7 @@ __device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid&
                                                const double* __restrict__ stages, const uint8_t* __restrict__ wc,
                                                const double* __restrict__ gh, double* __restrict__ r1,
                                                double* __restrict__ r23, double* __restrict__ r4, int nsbx, int tbx,
-                                               int tby) {
+                                               int tby, unsigned* fault = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int IN = TX * TY;
     extern __shared__ double4 smem_raw[];
@@ -648,7 +875,7 @@ __device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid&
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    load_windows<RH, RW, NT, BULK>(A, lam + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH);
+    if (!load_windows<RH, RW, NT, BULK>(A, lam + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH, fault)) return;
     const double dt = P.dt;
     const double c6 = dt / 6.0, c3 = dt / 3.0, c2 = dt * 0.5;
 #pragma unroll 2
@@ -680,9 +907,10 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
     k_adj_exact(DevModel P, DevGrid g, const double* __restrict__ lam, double* __restrict__ lamout,
                 const double* __restrict__ y, const double* __restrict__ stages, const uint8_t* __restrict__ wc,
                 const double* __restrict__ gh, double* __restrict__ r1, double* __restrict__ r23,
-                double* __restrict__ r4, int nsbx) {
+                double* __restrict__ r4, int nsbx, unsigned* fault) {
     pdl_enter();
-    adj_exact_tile<TX, TY, NT, true>(P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx, blockIdx.x, blockIdx.y);
+    adj_exact_tile<TX, TY, NT, true>(P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx, blockIdx.x, blockIdx.y,
+                                     fault);
 }
 
 // ---------------------------------------------------------------- batched
@@ -931,17 +1159,36 @@ TileShape tile_shape(int t) {
     }
 }
 
-cudaError_t take_device_fault(cudaStream_t st, unsigned* fault) {
+cudaError_t take_device_fault(cudaStream_t st, unsigned* d_fault, unsigned* fault) {
     unsigned v = 0;
-    cudaError_t e = cudaMemcpyFromSymbolAsync(&v, g_device_fault, sizeof v, 0, cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaMemcpyAsync(&v, d_fault, sizeof v, cudaMemcpyDeviceToHost, st);
     if (!e) e = cudaStreamSynchronize(st);
     if (!e && v) {
-        const unsigned zero = 0;
-        e = cudaMemcpyToSymbolAsync(g_device_fault, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, st);
+        e = cudaMemsetAsync(d_fault, 0, sizeof v, st);
         if (!e) e = cudaStreamSynchronize(st);
     }
     *fault = v;
     return e;
+}
+
+// Tile presets of the fused reference adjoint (TX, TY, threads): one CTA per
+// SM (its shared memory), TY a multiple of 16 (the z.gh sub-block sums).
+#define FKADJ_FUSED_LIST(X) \
+    X(0, 32, 32, 512)       \
+    X(1, 64, 16, 512)       \
+    X(2, 32, 32, 384)       \
+    X(3, 48, 16, 384)
+
+int fused_count() { return 4; }
+
+TileShape fused_shape(int t) {
+    switch (t) {
+#define X(id, a, b, c) \
+    case id: return {a, b, c};
+        FKADJ_FUSED_LIST(X)
+#undef X
+        default: return {32, 32, 512};
+    }
 }
 
 cudaError_t kernels_init() {
@@ -950,8 +1197,15 @@ cudaError_t kernels_init() {
     if ((e = setup_tile<a, b, c>()) != cudaSuccess) return e;
     FKADJ_TILE_LIST(X)
 #undef X
+#define X(id, a, b, c)                                                                                  \
+    if ((e = cudaFuncSetAttribute(k_adj_fused<a, b, c>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)fused_smem_bytes<a, b>())) != cudaSuccess)                        \
+        return e;
+    FKADJ_FUSED_LIST(X)
+#undef X
     return cudaSuccess;
 }
+
 
 // Launches a step kernel with programmatic stream serialisation (the kernel
 // starts with pdl_enter()).  FKADJ_NO_PDL=1 in the environment launches them
@@ -1003,11 +1257,12 @@ static dim3 tile_grid(const DevGrid& g, int tx, int ty) {
 }
 
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
-                            const double* gh, const EStep& E, cudaStream_t st, double* stages, int ty, double* k1) {
+                            const double* gh, const EStep& E, cudaStream_t st, unsigned* fault, double* stages, int ty,
+                            double* k1) {
     DISPATCH(tile, {
         const int rows = (ty > 0 && ty < TY) ? ty : TY;
         const cudaError_t e = launch_pdl(k_fwd_step<TX, TY, NT>, tile_grid(g, TX, rows), NT,
-                                         stencil_smem<TX, TY>(NT), st, P, g, yin, yout, gh, E, stages, rows, k1);
+                                         stencil_smem<TX, TY>(NT), st, P, g, yin, yout, gh, E, stages, rows, k1, fault);
         if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
@@ -1015,10 +1270,10 @@ cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const
 
 cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, const double* lam, double* lamout,
                              const double* y, const double* stages, const uint8_t* wc, const double* gh,
-                             double* r1, double* r23, double* r4, int nsbx, cudaStream_t st) {
+                             double* r1, double* r23, double* r4, int nsbx, cudaStream_t st, unsigned* fault) {
     DISPATCH(tile, {
         const cudaError_t e = launch_pdl(k_adj_exact<TX, TY, NT>, tile_grid(g, TX, TY), NT, exact_smem<TX, TY>(), st,
-                                         P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx);
+                                         P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx, fault);
         if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
@@ -1026,11 +1281,11 @@ cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, cons
 
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, const EStep& E, const HermiteW& hw, cudaStream_t st,
-                           const double* fin, double* fout, double* jh, int ty, const double* fa) {
+                           unsigned* fault, const double* fin, double* fout, double* jh, int ty, const double* fa) {
     DISPATCH(tile, {
         const int rows = (ty > 0 && ty < TY) ? ty : TY;
         const cudaError_t e = launch_pdl(k_adj_mid<TX, TY, NT>, tile_grid(g, TX, rows), NT, mid_smem<TX, TY>(), st,
-                                         P, g, ya, yb, gh, yh, E, hw, fin, fout, jh, rows, fa);
+                                         P, g, ya, yb, gh, yh, E, hw, fin, fout, jh, rows, fa, fault);
         if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
@@ -1065,13 +1320,32 @@ int balanced_rows(int tile, int kind, const DevGrid& g) {
 
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
-                            const double* gh, double* row, int nsbx, cudaStream_t st, const double* jb,
-                            const double* jh, double* ja) {
+                            const double* gh, double* row, int nsbx, cudaStream_t st, unsigned* fault,
+                            const double* jb, const double* jh, double* ja) {
     DISPATCH(tile, {
         const cudaError_t e = launch_pdl(k_adj_step<TX, TY, NT>, tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT),
-                                         st, P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja);
+                                         st, P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, fault);
         if (e != cudaSuccess) return e;
     });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_fused(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
+                             const double* ya, const double* yb, const double* fa, const double* fb, double* fout,
+                             const uint8_t* wc, const double* gh, const EStep& E, const HermiteW& hw, double* row,
+                             int nsbx, const double* jb, double* ja, cudaStream_t st, unsigned* fault) {
+    switch (tile) {
+#define X(id, a, b, c)                                                                                        \
+    case id: {                                                                                                \
+        const cudaError_t e = launch_pdl(k_adj_fused<a, b, c>, tile_grid(g, a, b), c, fused_smem_bytes<a, b>(), \
+                                         st, P, g, z, zout, ya, yb, fa, fb, fout, wc, gh, E, hw, row, nsbx, jb,  \
+                                         ja, fault);                                                           \
+        if (e != cudaSuccess) return e;                                                                       \
+    } break;
+        FKADJ_FUSED_LIST(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -97,17 +97,21 @@ int batch_preset(int tile);
 TileShape tile_shape(int tile);
 int tiles_of(int tile, const DevGrid& g);
 cudaError_t kernels_init();
-// Reads and clears the flag a kernel sets when one of its bounded waits
-// expires (after synchronising st); *fault != 0 means results are invalid.
-cudaError_t take_device_fault(cudaStream_t st, unsigned* fault);
+// Reads and clears a problem's fault word d_fault, which the step kernels set
+// when one of their bounded waits expires (after synchronising st); *fault != 0
+// means the results since the last check are invalid.  Every problem has its
+// own word, so problems running at once on other streams or host threads
+// neither see nor clear each other's faults.
+cudaError_t take_device_fault(cudaStream_t st, unsigned* d_fault, unsigned* fault);
 
 // ty: rows per tile, 0 < ty < the preset's height, or 0 for the preset's
 // height (forward step and adjoint midpoint only).  k1 (forward step): where
 // k1 = f(y, E0) is kept (a state, null = not kept).  fa (midpoint): f(ya, Ea)
-// as kept by the forward step from ya (null = evaluate).
+// as kept by the forward step from ya (null = evaluate).  fault: the launching
+// problem's fault word (device memory; null = not reported).
 cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const double* yin, double* yout,
-                            const double* gh, const EStep& E, cudaStream_t st, double* stages = nullptr, int ty = 0,
-                            double* k1 = nullptr);
+                            const double* gh, const EStep& E, cudaStream_t st, unsigned* fault,
+                            double* stages = nullptr, int ty = 0, double* k1 = nullptr);
 // Programmatic dependent launch for the step kernels issued by this thread
 // (on by default; the engine turns it off while it captures a graph).
 void set_launch_pdl(bool on);
@@ -121,17 +125,30 @@ int balanced_rows(int tile, int kind, const DevGrid& g);
 void subblock_lattice(const DevGrid& g, int* nsbx, int* nsby);
 cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, const double* lam, double* lamout,
                              const double* y, const double* stages, const uint8_t* wc, const double* gh,
-                             double* r1, double* r23, double* r4, int nsbx, cudaStream_t st);
+                             double* r1, double* r23, double* r4, int nsbx, cudaStream_t st, unsigned* fault);
 cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const double* ya, const double* yb,
                            const double* gh, double* yh, const EStep& E, const HermiteW& hw, cudaStream_t st,
-                           const double* fin = nullptr, double* fout = nullptr, double* jh = nullptr, int ty = 0,
-                           const double* fa = nullptr);
+                           unsigned* fault, const double* fin = nullptr, double* fout = nullptr,
+                           double* jh = nullptr, int ty = 0, const double* fa = nullptr);
 // jb: cached J(y_i) (null = evaluate), jh: cached J(yh) (null = evaluate),
 // ja: where J(y_{i-1}) is stored for the next step (null = not kept).
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
-                            const double* gh, double* row, int nsbx, cudaStream_t st, const double* jb = nullptr,
-                            const double* jh = nullptr, double* ja = nullptr);
+                            const double* gh, double* row, int nsbx, cudaStream_t st, unsigned* fault,
+                            const double* jb = nullptr, const double* jh = nullptr, double* ja = nullptr);
+// Fused reference-adjoint step (k_adj_mid and k_adj_step in one launch):
+// z -> zout over step [t_{i-1}, t_i] with ya = y_{i-1}, yb = y_i; fa, fb =
+// f(ya, Et[i-1]), f(yb, Et[i]) where kept or carried (null = evaluated), fout
+// (null = not kept) receives f(ya) when it was evaluated; E = (Et[i-1], Et[i],
+// E(t_{i-1} + dt/3)); jb = cached J_F(y_i)^T (null = evaluated), ja = where
+// J_F(y_{i-1})^T is stored for the next step (null = not stored).
+// tile: 0 .. fused_count()-1 (fused_shape).
+int fused_count();
+TileShape fused_shape(int tile);
+cudaError_t launch_adj_fused(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
+                             const double* ya, const double* yb, const double* fa, const double* fb, double* fout,
+                             const uint8_t* wc, const double* gh, const EStep& E, const HermiteW& hw, double* row,
+                             int nsbx, const double* jb, double* ja, cudaStream_t st, unsigned* fault);
 cudaError_t launch_dot_gh(const DevGrid& g, const double* z, const double* gh, double* row, int nsbx, int nsby,
                           cudaStream_t st);
 cudaError_t launch_sum_rows(const double* partial, int rows, int ntiles, double* out, cudaStream_t st);

@@ -15,7 +15,10 @@
 // array's name as a device address (it denotes a host-side stand-in), so the
 // first call on each device, with that device current, resolves the address
 // with cudaGetSymbolAddress and caches it; that first call should therefore
-// come before any stream capture.  Every later call on the device re-uses the
+// come before any stream capture.  The cached address belongs to the device's
+// primary context of that moment: after cudaDeviceReset (or any teardown and
+// re-creation of the primary context) it is stale, and the entry point must
+// not be called again in the process.  Every later call on the device re-uses the
 // same array: calls that overlap on the GPU (other streams, other host
 // threads) race on it and must be serialised by the caller.  Each call writes
 // every partial it later reads, so nothing has to start at zero and the array

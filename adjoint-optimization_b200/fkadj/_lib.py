@@ -27,7 +27,8 @@ EXPORTS = (
     "fkadj_problem_destroy",
     "fkadj_problem_device_bytes", "fkadj_problem_objective", "fkadj_problem_grad",
     "fkadj_problem_last_timing", "fkadj_problem_last_launches", "fkadj_problem_set_profiling",
-    "fkadj_problem_kernel_time", "fkadj_problem_tiles",
+    "fkadj_problem_kernel_time", "fkadj_problem_tiles", "fkadj_problem_last_plan",
+    "fkadj_problem_adjoint_kernel",
 )
 
 
@@ -80,6 +81,8 @@ def load():
     L.fkadj_problem_set_profiling.argtypes = [C.c_void_p, C.c_int]
     L.fkadj_problem_kernel_time.argtypes = [C.c_void_p, C.c_int, dp, i64p]
     L.fkadj_problem_tiles.argtypes = [C.c_void_p, ip, ip]
+    L.fkadj_problem_last_plan.argtypes = [C.c_void_p, i64p]
+    L.fkadj_problem_adjoint_kernel.argtypes = [C.c_void_p, ip]
     for name in ("fkadj_forward", "fkadj_grad", "fkadj_problem_create", "fkadj_problem_objective",
                  "fkadj_problem_grad"):
         getattr(L, name).restype = C.c_int

@@ -182,6 +182,24 @@ class Problem:
     def last_launches(self) -> int:
         return int(self._L.fkadj_problem_last_launches(self._h))
 
+    @property
+    def last_plan(self):
+        """Trajectory store of the last gradient: policy (FULL/SQRT/BINOMIAL
+        name), stored slots, segment/scratch slots, recomputed forward steps."""
+        out = (C.c_int64 * 4)()
+        self._L.fkadj_problem_last_plan(self._h, out)
+        names = {0: None, _lib.CKPT_FULL: "full", _lib.CKPT_SQRT: "sqrt", _lib.CKPT_BINOMIAL: "binomial"}
+        return {"policy": names.get(int(out[0]), int(out[0])), "slots": int(out[1]), "segment_slots": int(out[2]),
+                "recompute_steps": int(out[3])}
+
+    @property
+    def adjoint_kernel(self):
+        """The reference-mode backward step: path ("split", "fused" with the
+        J cache, "fused-recompute") and the fused kernel's (TX, TY, threads)."""
+        out = (C.c_int * 4)()
+        self._L.fkadj_problem_adjoint_kernel(self._h, out)
+        return {"path": ("split", "fused", "fused-recompute")[out[0]], "tile": (out[1], out[2], out[3])}
+
     def set_profiling(self, on: bool = True) -> None:
         self._L.fkadj_problem_set_profiling(self._h, 1 if on else 0)
 

@@ -64,11 +64,11 @@ def _batch_insts(a):
     return W.batch_instances(count=a.count, seed=a.seed, max_side=a.max_side, nt_scale=a.nt_scale)
 
 
-def cmd_batch(a):
-    insts = _batch_insts(a)
+def batch_measure(insts):
+    """Gradients of `insts` one resident problem at a time (created, warmed,
+    timed, freed; the timed call replays the gradient's captured graph) and all
+    of them as one batch; wall times and throughputs."""
     cells_steps = sum(i.nrows * i.ncols * i.nt for i in insts)
-    # one resident problem at a time (created, warmed, timed, freed); two warm-up
-    # calls, so the timed call replays the captured graph of the gradient
     seq = 0.0
     for inst in insts:
         with api.Problem(inst, opts=api.options(ckpt_policy=_lib.CKPT_SQRT)) as pb:
@@ -88,24 +88,28 @@ def cmd_batch(a):
         [b.result(j) for j in jobs]
         bt = time.perf_counter() - t0
         st = b.stats
-    print(json.dumps({"suite": "batch", "count": a.count, "max_side": a.max_side, "nt_scale": a.nt_scale,
-                      "uniform": getattr(a, "side", 0) > 0,
-                      "sides": sorted({i.nrows for i in insts}), "nt_range": [min(i.nt for i in insts),
-                                                                              max(i.nt for i in insts)],
-                      "sequential_s": seq, "batched_s": bt, "speedup": seq / bt,
-                      "gradients_per_s_sequential": a.count / seq, "gradients_per_s_batched": a.count / bt,
-                      "cell_steps_per_s_batched": cells_steps / bt, "ticks": st["ticks"],
-                      "launches": st["launches"], "device_bytes": st["device_bytes"]}), flush=True)
+    n = len(insts)
+    return {"count": n, "sides": sorted({i.nrows for i in insts}),
+            "nt_range": [min(i.nt for i in insts), max(i.nt for i in insts)],
+            "sequential_s": seq, "batched_s": bt, "speedup": seq / bt,
+            "gradients_per_s_sequential": n / seq, "gradients_per_s_batched": n / bt,
+            "cell_steps_per_s_batched": cells_steps / bt, "ticks": st["ticks"], "launches": st["launches"],
+            "device_bytes": st["device_bytes"]}
 
 
-def cmd_serve(a):
-    rng = np.random.default_rng(a.seed)
-    base = _batch_insts(argparse.Namespace(count=a.requests, seed=a.seed, max_side=a.max_side,
-                                           nt_scale=a.nt_scale))
-    grads = [bool(x) for x in rng.integers(0, 2, size=a.requests)]
-    # standalone service time of every request, two ways: a plain solve of a new
-    # instance (problem set-up, upload, autotune and the call: what one request
-    # costs without the server) and a warm resident call (set-up excluded)
+def cmd_batch(a):
+    out = batch_measure(_batch_insts(a))
+    out.update({"suite": "batch", "max_side": a.max_side, "nt_scale": a.nt_scale, "uniform": getattr(a, "side", 0) > 0})
+    print(json.dumps(out), flush=True)
+
+
+def serve_measure(base, grads, rates, rng):
+    """A stream of requests (instances `base`, objective+gradient where
+    grads[k]) at each Poisson rate: latency p50/p99 and throughput served by
+    the continuous-batching server, against the same arrivals solved one at a
+    time in arrival order (FIFO) as plain solves of new instances (problem
+    set-up, upload and the call: what a request costs without the server) and
+    as warm resident calls (set-up excluded)."""
     service, service_warm = [], []
     for inst, g in zip(base, grads):
         t0 = time.perf_counter()
@@ -116,8 +120,10 @@ def cmd_serve(a):
             t0 = time.perf_counter()
             (pb.grad if g else pb.objective)(inst.Et)
             service_warm.append(time.perf_counter() - t0)
-    for rate in a.rates:
-        gaps = rng.exponential(1.0 / rate, size=a.requests)
+    n = len(base)
+    out = []
+    for rate in rates:
+        gaps = rng.exponential(1.0 / rate, size=n)
         arrive = np.cumsum(gaps) - gaps[0]
         with Server(opts=api.options(ckpt_policy=_lib.CKPT_SQRT)) as srv:
             t0 = time.perf_counter()
@@ -133,24 +139,39 @@ def cmd_serve(a):
                 lat.append(srv.result(rid)["latency_s"])
             makespan = time.perf_counter() - t0
             peak = srv.stats["peak_running"]
-        # sequential FIFO plain solves with the same arrivals
+
         def fifo(svc):
-            fin, out = 0.0, []
-            for k in range(a.requests):
+            fin, res = 0.0, []
+            for k in range(n):
                 fin = max(arrive[k], fin) + svc[k]
-                out.append(fin - arrive[k])
-            return fin, out
+                res.append(fin - arrive[k])
+            return fin, res
         fin, seq_lat = fifo(service)
         fin_w, seq_w = fifo(service_warm)
-        print(json.dumps({"suite": "serve", "rate_req_s": rate, "requests": a.requests,
-                          "max_side": a.max_side, "nt_scale": a.nt_scale,
-                          "served_p50_s": _pct(lat, 50), "served_p99_s": _pct(lat, 99),
-                          "served_throughput_req_s": a.requests / makespan,
-                          "sequential_p50_s": _pct(seq_lat, 50), "sequential_p99_s": _pct(seq_lat, 99),
-                          "sequential_throughput_req_s": a.requests / fin,
-                          "sequential_warm_p50_s": _pct(seq_w, 50), "sequential_warm_p99_s": _pct(seq_w, 99),
-                          "sequential_warm_throughput_req_s": a.requests / fin_w,
-                          "peak_running": peak}), flush=True)
+        out.append({"rate_req_s": rate, "requests": n,
+                    "served_p50_s": _pct(lat, 50), "served_p99_s": _pct(lat, 99),
+                    "served_throughput_req_s": n / makespan,
+                    "sequential_p50_s": _pct(seq_lat, 50), "sequential_p99_s": _pct(seq_lat, 99),
+                    "sequential_throughput_req_s": n / fin,
+                    "sequential_warm_p50_s": _pct(seq_w, 50), "sequential_warm_p99_s": _pct(seq_w, 99),
+                    "sequential_warm_throughput_req_s": n / fin_w, "peak_running": peak})
+    return out
+
+
+def serve_requests(requests, seed, max_side, nt_scale):
+    """The request mix of the served stream: sizes and horizons as the uneven
+    batch (fkadj.workloads.batch_instances), half of them objective+gradient."""
+    rng = np.random.default_rng(seed)
+    base = _batch_insts(argparse.Namespace(count=requests, seed=seed, max_side=max_side, nt_scale=nt_scale))
+    grads = [bool(x) for x in rng.integers(0, 2, size=requests)]
+    return base, grads, rng
+
+
+def cmd_serve(a):
+    base, grads, rng = serve_requests(a.requests, a.seed, a.max_side, a.nt_scale)
+    for r in serve_measure(base, grads, a.rates, rng):
+        r.update({"suite": "serve", "max_side": a.max_side, "nt_scale": a.nt_scale})
+        print(json.dumps(r), flush=True)
 
 
 def cmd_opt(a):

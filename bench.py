@@ -12,14 +12,16 @@ layouts (the reference publishes no benchmark).
           (CUDA events on the engine's stream), max over ranks, x ranks
   e2e     the same metric through the drop-in C-ABI call fkadj_grad with host
           buffers (pinned), host<->device copies inside the timed region
-  roofline  the dominant kernel's algorithmic bytes / its average launch time
-          (sampled CUDA events inside the engine, same process, right after
-          the timed region) against MEASURED_PEAKS.json's HBM copy bandwidth
+  roofline  the dominant kernel's algorithmic bytes (and FP64 flops) / its
+          average launch time (CUDA events on the engine stream) against
+          MEASURED_PEAKS.json's HBM copy bandwidth (and the FP64 peak); the
+          roof with the larger fraction leads the block
   cpu_baseline  the CPU oracle (C, OpenMP, all host cores) on a bounded
           sample of the same workload, scaled to gradients/s
 
 --impl reference times the reference algorithm on the host cores (the CPU
-oracle port; the reference's own code runs through MATLAB, absent here).
+oracle port; the reference's own code runs through MATLAB, absent here), one
+bounded sample of the workload per timed step.
 Multi-GPU: independent replicas (one instance per rank, no collective on the
 data path); torch.distributed/NCCL only for the barrier and the max.
 """
@@ -50,16 +52,16 @@ BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
                   2: 249.0}   # adjoint step: read z (24) + J(y_i), J(yh) (112) + y_{i-1} (24) + gh (8)
                               #   + weight code (1), write z (24) + J(y_{i-1}) (56)
 # DRAM bytes per cell of one k_fwd_step launch measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, caches flushed before the launch) at 512x512:
-# profiles/k_fwd_step_512x512_traffic.md.  The reads (33 B/cell: y 24 + gh 8 +
-# halo) reach DRAM; the 24 B/cell of writes stay in the 126 MB L2.
+# dram__bytes_write.sum, caches flushed before the launch) at 512x512.  The reads
+# (33 B/cell: y 24 + gh 8 + halo) reach DRAM; the 24 B/cell of writes stay in the
+# 126 MB L2.
 FWD_TRAFFIC_PER_CELL = 8656640 / 262144
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
 # discrete-exact adjoint step (--mode exact): read lambda (24), y (24), the three stage states (72), gh (8),
 # weight code (1); write lambda (24)
 EXACT_BYTES_PER_CELL = 153.0
 # FP64 flops per vector-field evaluation of the forward step (stage update included), counted by ncu
-# (2 x DFMA + DMUL + DADD thread instructions): profiles/fp64_ops_512x512.md
+# (2 x DFMA + DMUL + DADD thread instructions) at 512x512
 FWD_FLOPS_PER_EVAL = 740.4 / 4.58984375
 
 
@@ -147,6 +149,26 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def binding_roof(roof):
+    """The roofline block led by the roof the kernel is nearer to: the HBM
+    fraction (algorithmic bytes / copy bandwidth) and the FP64 fraction (flops /
+    nominal FP64 peak) are both measured on the same launches; the larger one
+    binds and takes the top-level fields, the other stays as a sub-block."""
+    fp = roof.get("fp64")
+    if not fp or fp["kernel"] != roof["kernel"] or fp["frac"] <= roof["frac"]:
+        return roof
+    hbm = {k: roof[k] for k in ("kernel", "achieved", "peak", "unit", "frac", "peak_source", "traffic",
+                                "bytes_per_launch", "avg_launch_ms") if k in roof}
+    out = {k: v for k, v in roof.items() if k not in hbm and k != "fp64"}
+    out.update({"bound": "fp64", "kernel": fp["kernel"], "achieved": fp["achieved"], "peak": fp["peak"],
+                "unit": fp["unit"], "frac": fp["frac"], "peak_source": fp["peak_source"],
+                "traffic": roof.get("traffic"), "flops_per_launch": fp["flops_per_launch"],
+                "avg_launch_ms": fp["avg_launch_ms"], "flops_source": fp["flops_source"], "hbm": hbm})
+    if "traffic_source" in roof:
+        out["traffic_source"] = roof["traffic_source"]
+    return out
+
+
 def workload(args):
     from fkadj import workloads as W
     inst = W.large_instance(n=args.n, nt=args.nt, seed=1)
@@ -178,26 +200,40 @@ def cpu_sample(args, inst, steps=None):
            inst.active_index, obj, inst.alpha, mode="ref")
     dt = time.perf_counter() - t0
     per_grad = dt * inst.nt / nts
-    return {"value": 1.0 / per_grad, "unit": UNIT, "cores": O.threads(), "kind": "port",
+    return {"value": 1.0 / per_grad, "unit": UNIT, "cores": O.threads(), "kind": "port", "sample_s": dt,
             "sample": f"{inst.nrows}x{inst.ncols} grid, {nts} fwd+adjoint steps ({dt:.1f} s) scaled to "
                       f"{inst.nt} steps; C oracle, OpenMP"}
 
 
 def run_reference(args):
+    """The reference algorithm on the host cores.  Each of the K timed steps is
+    one bounded sample of the workload: args.ref_sample_steps of its nt RK4
+    steps, forward then adjoint, on the same grid (the full 20000-step gradient
+    takes about five minutes on 16 cores).  ms_per_step is the wall time of one
+    sample, so steps x ms_per_step is the timed run; value scales each sample to
+    whole gradients (per-step cost does not depend on the horizon)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     inst = workload(args)
-    if args.warmup > 0:
+    for _ in range(args.warmup):
         cpu_sample(args, inst, steps=4)  # untimed: pages the oracle and its buffers in
-    vals = [cpu_sample(args, inst) for _ in range(max(1, args.steps if args.steps <= 2 else 2))]
-    v = statistics.median([x["value"] for x in vals])
-    cb = dict(vals[0])
+    samples = [cpu_sample(args, inst, steps=args.ref_sample_steps) for _ in range(max(1, args.steps))]
+    sample_s = [x["sample_s"] for x in samples]
+    per_sample = statistics.median(sample_s)
+    v = statistics.median([x["value"] for x in samples])
+    cb = dict(samples[0])
     cb["value"] = v
+    cb.pop("sample_s", None)
+    config = workload_config(args, inst, "full (host)")
+    config["timed_step"] = (f"one sample of {args.ref_sample_steps} of the {inst.nt} RK4 steps (forward + "
+                            f"adjoint), scaled to whole gradients")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "steps": len(samples), "warmup": args.warmup, "ms_per_step": 1000.0 * per_sample,
+            "sample_steps": args.ref_sample_steps, "extrapolated_to": inst.nt,
+            "timed_s": sum(sample_s), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(args, inst, "full (host)"), "cpu_baseline": cb,
+            "config": config, "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -330,10 +366,11 @@ def run_ours(args):
     roof["fp64"] = {"kernel": "k_fwd_step", "achieved": fl / (fwd_live_ms / 1000.0) / 1e12, "peak": fpeak,
                     "unit": "TFLOP/s", "frac": fl / (fwd_live_ms / 1000.0) / 1e12 / fpeak, "avg_launch_ms": fwd_live_ms,
                     "flops_per_launch": fl, "peak_source": "148 SMs x 64 DFMA/clock x 2 at the sampled SM clock",
-                    "flops_source": "ncu-counted FP64 instructions per evaluation, profiles/fp64_ops_512x512.md"}
+                    "flops_source": "ncu-counted FP64 instructions per evaluation at 512x512"}
     if roof["traffic"] is None and dom == 0 and FWD_TRAFFIC_PER_CELL:
         roof["traffic"] = FWD_TRAFFIC_PER_CELL * cells
-        roof["traffic_source"] = "ncu capture, profiles/k_fwd_step_512x512_traffic.md"
+        roof["traffic_source"] = "ncu capture of one k_fwd_step launch at 512x512 (dram read + write)"
+    roof = binding_roof(roof)
     sqrt_bytes = pb.device_bytes
     pb.close()
 
@@ -358,6 +395,27 @@ def run_ours(args):
         except _lib.FkadjError as e:
             full = {"unavailable": str(e)}
 
+    # the same gradient with the store AUTO picks within the default budget (60% of free memory)
+    auto = None
+    if not args.no_auto and args.ckpt != "auto" and world == 1:
+        try:
+            aopts = api.options(ckpt_policy=_lib.CKPT_AUTO, stream=stream.cuda_stream, device=local, tile=args.tile,
+                                grad_mode=gmode)
+            with api.Problem(inst, opts=aopts) as pa:
+                pa.grad(Et, inst.y0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for _ in range(args.full_steps):
+                    pa.grad(Et)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ams = e0.elapsed_time(e1) / args.full_steps
+                auto = {"value": 1000.0 / ams, "unit": UNIT, "ms_per_step": ams, "steps": args.full_steps,
+                        "device_bytes": pa.device_bytes, **pa.last_plan}
+        except _lib.FkadjError as e:
+            auto = {"unavailable": str(e)}
+
     # e2e through the drop-in C ABI (fkadj_grad), host buffers in pinned memory
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     Et_h, y0_h = pin(inst.Et), pin(inst.y0)
@@ -380,9 +438,16 @@ def run_ours(args):
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
            "path": "fkadj_grad (drop-in for fk_grad_Et_comp), one call per gradient incl. device setup"}
 
+    # the metric's second half: served p50/p99 against plain solves, and the
+    # batched uneven instances, at a stated scale-down of their workloads
+    served = plain = batched = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        served, plain, batched = serve_and_batch(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(args, inst)
+        cpu.pop("sample_s", None)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -391,9 +456,43 @@ def run_ours(args):
                 "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
         if full is not None:
             line["full_storage"] = full
+        if auto is not None:
+            line["auto_store"] = auto
+        if served is not None:
+            line["served"], line["plain_solve"], line["batched"] = served, plain, batched
         print(json.dumps(line), flush=True)
     ranks.close()
     return 0
+
+
+def serve_and_batch(args):
+    """Served stream and batched uneven instances (scaled down from the
+    standard 128-1024 sides and 1000-20000 steps so the bench stays within
+    minutes; the keys say how)."""
+    from fkadj import suite
+    from fkadj import workloads as W
+    base, grads, rng = suite.serve_requests(args.serve_requests, 7, args.serve_max_side, args.serve_nt_scale)
+    rows = suite.serve_measure(base, grads, args.serve_rates, rng)
+    mix = {"requests": args.serve_requests, "objective_and_gradient": int(sum(grads)),
+           "sides": sorted({i.nrows for i in base}), "nt_range": [min(i.nt for i in base), max(i.nt for i in base)],
+           "arrivals": "Poisson", "scale": f"sides <= {args.serve_max_side}, horizons x{args.serve_nt_scale} of "
+                                           f"the 128-1024 / 1000-20000-step mix", "timer": "host wall clock"}
+    served = dict(mix, rates=[{"rate_req_s": r["rate_req_s"], "p50_s": r["served_p50_s"], "p99_s": r["served_p99_s"],
+                               "throughput_req_s": r["served_throughput_req_s"], "peak_running": r["peak_running"]}
+                              for r in rows])
+    plain = dict(mix, what="the same arrivals solved one at a time in arrival order, each a plain "
+                           "single-instance solve of a new problem (set-up, upload, call)",
+                 rates=[{"rate_req_s": r["rate_req_s"], "p50_s": r["sequential_p50_s"], "p99_s": r["sequential_p99_s"],
+                         "throughput_req_s": r["sequential_throughput_req_s"],
+                         "warm_p50_s": r["sequential_warm_p50_s"], "warm_p99_s": r["sequential_warm_p99_s"]}
+                        for r in rows])
+    insts = W.batch_instances(count=args.batch_count, seed=2, max_side=args.serve_max_side,
+                              nt_scale=args.serve_nt_scale)
+    batched = suite.batch_measure(insts)
+    batched["scale"] = (f"{args.batch_count} of the 64 uneven instances, sides <= {args.serve_max_side}, "
+                        f"horizons x{args.serve_nt_scale}")
+    batched["sequential"] = "one resident problem at a time, each gradient a replayed graph"
+    return served, plain, batched
 
 
 def pb_stride(nt):
@@ -414,10 +513,19 @@ def main():
                     help="gradient mode: the reference's continuous adjoint (the headline) or the discrete-exact one")
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cpu-steps", type=int, default=600)
+    ap.add_argument("--ref-sample-steps", type=int, default=300,
+                    help="reference arm: RK4 steps (forward + adjoint) timed per step of the run")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-full", action="store_true", help="skip the full-trajectory comparison")
     ap.add_argument("--full-steps", type=int, default=2)
+    ap.add_argument("--no-auto", action="store_true", help="skip the AUTO-store comparison")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream and batched measurements")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-rates", type=lambda x: [float(v) for v in x.split(",")], default=[10.0, 50.0, 200.0])
+    ap.add_argument("--serve-max-side", type=int, default=512)
+    ap.add_argument("--serve-nt-scale", type=float, default=0.1)
+    ap.add_argument("--batch-count", type=int, default=16)
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if captured")
     args = ap.parse_args()

@@ -65,7 +65,8 @@ typedef enum {
 } fkadj_grad_mode;
 
 typedef enum {
-    FKADJ_CKPT_AUTO = 0,     /* FULL when it fits the budget, else SQRT, else BINOMIAL */
+    FKADJ_CKPT_AUTO = 0,     /* FULL when it fits the budget, else whichever of SQRT and
+                                BINOMIAL fits and recomputes fewer forward steps */
     FKADJ_CKPT_FULL = 1,     /* every state resident on the device */
     FKADJ_CKPT_SQRT = 2,     /* ~sqrt(nt) checkpoints, segments recomputed backward */
     FKADJ_CKPT_BINOMIAL = 3  /* binomial (revolve) schedule within ckpt_budget_bytes */
@@ -156,6 +157,22 @@ void fkadj_problem_last_timing(const fkadj_problem *pb, double out[3]);
 
 /* Number of kernel launches the last call on the problem issued. */
 int64_t fkadj_problem_last_launches(const fkadj_problem *pb);
+
+/* Trajectory store of the last gradient on the problem (no counterpart in the
+ * reference, which keeps every state in host memory, cu-G:1658-1664):
+ * out[0] policy (fkadj_ckpt_policy FULL/SQRT/BINOMIAL; 0 before the first
+ * gradient), out[1] stored state slots, out[2] segment / scratch slots,
+ * out[3] forward steps the backward sweep recomputes. */
+void fkadj_problem_last_plan(const fkadj_problem *pb, int64_t out[4]);
+
+/* How the reference-mode backward step runs (no counterpart in the reference,
+ * which launches seven kernels per step, cu-G:1874-1895): out[0] 0 = midpoint
+ * and step kernels, 1 = one fused kernel reading the cached J_F(y)^T, 2 = one
+ * fused kernel evaluating it; out[1..3] the fused kernel's tile (TX, TY,
+ * threads), 0 for the split kernels (fkadj_problem_tiles has theirs).  Chosen
+ * by the autotuner at the first gradient unless FKADJ_ADJ_PATH (split, fused,
+ * fused-recompute) fixes it. */
+void fkadj_problem_adjoint_kernel(const fkadj_problem *pb, int out[4]);
 
 /* Sampled per-kernel device time: when enabled, CUDA events bracket about one
  * in (nt/100) launches of each kernel kind during the following calls.
@@ -251,7 +268,10 @@ void fkadj_server_stats(fkadj_server *s, int64_t out[6]);
  * The partial sums use a fixed device array of FKADJ_NOALLOC_MAX_SUBBLOCKS
  * 16x16 sub-blocks (512 KiB, held by every GPU that loads the library until
  * exit); larger grids are rejected with FKADJ_ERR_ARG.  The first call on a
- * device resolves that array's address (make it before any stream capture).
+ * device resolves that array's address (make it before any stream capture)
+ * and the library keeps it for the life of the process: after cudaDeviceReset,
+ * or anything else that re-creates the device's primary context, it is stale
+ * and the entry point must not be called again in that process.
  * All calls on a device share the array: calls that overlap on the GPU race,
  * so the caller serialises them.  Nothing is allocated.
  * --------------------------------------------------------------------- */

@@ -23,6 +23,18 @@ def golden():
     return dict(np.load(GOLDEN))
 
 
+def reference_dir():
+    """The reference tree, where it is mounted: FKADJ_REFERENCE_DIR, else the
+    directory oracle/ref_build.sh recorded when it built oracle/_ref; None
+    when neither exists (a GPU box has no reference tree)."""
+    d = os.environ.get("FKADJ_REFERENCE_DIR")
+    if not d:
+        rec = os.path.join(ROOT, "oracle", "_ref", "source_dir")
+        if os.path.exists(rec):
+            d = open(rec).read().strip()
+    return d if d and os.path.isdir(d) else None
+
+
 def has_gpu():
     try:
         import torch

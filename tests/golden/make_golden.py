@@ -16,6 +16,7 @@ gamma=[1,.2,.2], final_time=300, h=0.035 (fk_parameters_00_05_alpha_0p8_dx_0p035
 
 Output: tests/golden/ref256.npz (compressed).  Usage:
     python tests/golden/make_golden.py [/path/to/reference]
+(default: FKADJ_REFERENCE_DIR, else the container's mount point)
 """
 import os
 import sys
@@ -23,7 +24,7 @@ import sys
 import numpy as np
 import scipy.io as sio
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FKADJ_REFERENCE_DIR", "/root/reference")
 D = os.path.join(REF, "src", "cuda", "data")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref256.npz")
 

@@ -37,12 +37,29 @@ def test_measured_peaks_file_is_read_when_present(tmp_path, monkeypatch):
 
 def test_reference_arm_prints_its_line_on_a_small_grid():
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "64",
-                          "--nt", "40", "--cpu-steps", "4", "--steps", "1", "--warmup", "1"],
+                          "--nt", "40", "--ref-sample-steps", "8", "--steps", "3", "--warmup", "1"],
                          cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["unit"] == "gradients/s" and line["value"] > 0
+    # each timed step is one sample of 8 of the 40 steps: steps x ms_per_step is the timed run
+    assert line["steps"] == 3 and line["sample_steps"] == 8 and line["extrapolated_to"] == 40
+    assert abs(line["steps"] * line["ms_per_step"] / 1000.0 - line["timed_s"]) <= 0.5 * line["timed_s"]
+    assert abs(line["value"] - 8 / 40 / (line["ms_per_step"] / 1000.0)) <= 0.5 * line["value"]
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": "gradients/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["grid"] == [64, 64] and line["config"]["nt"] == 40
+
+
+def test_binding_roof_leads_with_the_larger_fraction():
+    roof = {"bound": "hbm", "kernel": "k_fwd_step", "achieved": 850.0, "peak": 6500.0, "unit": "GB/s",
+            "frac": 850.0 / 6500.0, "peak_source": "measured", "traffic": 1.0, "bytes_per_launch": 2.0,
+            "avg_launch_ms": 0.017, "note": "x",
+            "fp64": {"kernel": "k_fwd_step", "achieved": 11.4, "peak": 37.2, "unit": "TFLOP/s", "frac": 11.4 / 37.2,
+                     "peak_source": "nominal", "flops_per_launch": 3.0, "avg_launch_ms": 0.017, "flops_source": "y"}}
+    out = bench.binding_roof(dict(roof))
+    assert out["bound"] == "fp64" and out["unit"] == "TFLOP/s" and out["frac"] == 11.4 / 37.2
+    assert out["hbm"]["frac"] == 850.0 / 6500.0 and out["hbm"]["unit"] == "GB/s" and "fp64" not in out
+    roof["fp64"]["frac"] = 0.01
+    assert bench.binding_roof(dict(roof))["bound"] == "hbm"

@@ -42,15 +42,16 @@ def probe(tmp_path_factory):
     lib.probe_bulk.restype = ctypes.c_int
     lib.probe_bulk.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.c_uint, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
-                               ctypes.POINTER(ctypes.c_float)]
+                               ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
 
-    def run(src, rows_alloc, ld, rows, col0, extra=0, limit_ns=1_000_000_000):
+    def run(src, rows_alloc, ld, rows, col0, extra=0, limit_ns=1_000_000_000, cta_mode=False, with_fault=False):
         out = np.full(3 * rows * WIDTH, np.nan)
-        status, ms = ctypes.c_int(-1), ctypes.c_float(0)
+        status, ms, fault = ctypes.c_int(-1), ctypes.c_float(0), ctypes.c_uint(7)
         rc = lib.probe_bulk(src.ctypes.data, rows_alloc, ld, rows, col0, extra, limit_ns, out.ctypes.data,
-                            ctypes.byref(status), ctypes.byref(ms))
+                            ctypes.byref(status), ctypes.byref(ms), 1 if cta_mode else 0, ctypes.byref(fault))
         assert rc == 0, f"CUDA error {rc}"
-        return out.reshape(3, rows, WIDTH), status.value, ms.value
+        r = (out.reshape(3, rows, WIDTH), status.value, ms.value)
+        return r + (fault.value,) if with_fault else r
 
     return run
 
@@ -80,4 +81,23 @@ def test_bounded_wait_expires_reports_and_leaves_the_context_usable(probe):
     assert 40.0 <= ms < 5000.0, ms              # after its limit, not forever
     out, status, _ = probe(src, rows_alloc, ld, 24, 0)  # the next call on the same context works
     assert status == 1
+    np.testing.assert_array_equal(out, src.reshape(3, rows_alloc, ld)[:, :24, :WIDTH])
+
+
+@pytest.mark.gpu
+def test_expired_wait_in_a_step_kernel_skips_the_tile_and_sets_the_fault_word(probe):
+    """The step kernels wait with bulk_wait_cta: when the wait expires the CTA
+    sets its problem's fault word, waits once more (bounded) and returns
+    before computing or storing anything; the next call is correct."""
+    rows_alloc, ld = 40, 80
+    src = _planes(rows_alloc, ld, 6)
+    limit_ns = 50_000_000
+    out, status, ms, fault = probe(src, rows_alloc, ld, 24, 0, extra=16, limit_ns=limit_ns, cta_mode=True,
+                                   with_fault=True)
+    assert fault == 1                           # the fault word passed to the kernel is set
+    assert status == -1                         # the CTA returned before it wrote its outcome ...
+    assert np.isnan(out).all()                  # ... or any of the window
+    assert 80.0 <= ms < 10000.0, ms             # two bounded waits, then out
+    out, status, ms, fault = probe(src, rows_alloc, ld, 24, 0, cta_mode=True, with_fault=True)
+    assert fault == 0 and status == 1
     np.testing.assert_array_equal(out, src.reshape(3, rows_alloc, ld)[:, :24, :WIDTH])

@@ -107,3 +107,38 @@ def test_zero_pulse(mode):
     inst = _custom(mask, 100, Et=np.zeros(101))
     _forward_matches(inst)
     _grad_matches(inst, mode)
+
+
+@pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
+def test_nonfinite_gradient_with_finite_objective_is_a_numeric_error(mode):
+    """The adjoint's z.gh sums overflow while y(T) and the objective stay
+    finite: the pulse is zero, so gh never enters the forward sweep, and one
+    active cell gets a ghost_lr near the largest double while gamma_u scales
+    z(T) = -gamma_u S u(T) past 1 there.  The objective-only call succeeds with
+    a finite J; the gradient call reports a numeric error instead of returning
+    an infinite gradient with FKADJ_OK.  The failure is made on the host (the
+    inputs); nothing on the GPU faults."""
+    mask = np.ones((48, 48), bool)
+    mask[20:24, 20:24] = False
+    inst = _custom(mask, 60, Et=np.zeros(61), objective="mean_u2", alpha=0.0)
+    _, yf, _ = api.fk_forward_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                                 inst.ghost, 0, params=inst.params)
+    uT = G.compact(yf, inst.active_index)[:inst.n_num]
+    k = int(np.argmax(np.abs(uT)))
+    assert abs(uT[k]) > 0.05
+    ghost = inst.ghost.astype(np.float64).copy()
+    ghost[k] = 1.7e308
+    gamma = np.array([1.0e5 * inst.n_num, 0.0, 0.0])
+    with api.Problem(params=inst.params, dt=inst.dt, nt=inst.nt, active_index=inst.active_index,
+                     nrows=inst.nrows, ncols=inst.ncols, ghost_lr=ghost, gamma=gamma, S=inst.S, alpha=0.0,
+                     opts=api.options(grad_mode=mode)) as pb:
+        r = pb.objective(inst.Et, inst.y0)
+        assert np.isfinite(r["Lcost"]) and r["Lcost"] > 0
+        with pytest.raises(FkadjError) as e:
+            pb.grad(inst.Et, inst.y0)
+        assert e.value.status == _lib.ERR_NUMERIC
+        assert "gradient is not finite" in str(e.value)
+    with pytest.raises(FkadjError) as e:
+        api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows, ghost, gamma,
+                       inst.S, 0.0, params=inst.params, opts=api.options(grad_mode=mode))
+    assert e.value.status == _lib.ERR_NUMERIC

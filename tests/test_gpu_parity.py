@@ -175,10 +175,11 @@ def _state_bytes(nrows, ncols):
 
 
 @pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
-@pytest.mark.parametrize("slots", [2, 4, 9])
+@pytest.mark.parametrize("slots", [2, 4, 9, 60])
 def test_binomial_checkpointing_equals_full_storage(mode, slots):
     """Binomial reversal with a budget of `slots` states (2 = no free snapshot,
-    every state replayed from y_0) gives the same bits as full storage."""
+    every state replayed from y_0; 60 = a long chain of checkpoints stored by
+    the forward sweep itself) gives the same bits as full storage."""
     inst = _inst(48, 70 if slots == 2 else 130, seed=23, ncols=64, objective="gradient")
     args = (inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows, inst.ghost,
             inst.gamma, inst.S, 0.2)
@@ -212,3 +213,28 @@ def test_windowed_zgh_reduction_matches_oracle_and_batch(mode):
                inst.active_index, O.Objective(inst.S, inst.gamma), inst.alpha,
                mode="ref" if mode == _lib.GRAD_REF else "exact")
     assert np.linalg.norm(g - o["gradE"]) <= 1e-8 * np.linalg.norm(o["gradE"])
+
+
+@pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
+def test_auto_store_takes_the_schedule_that_recomputes_less(mode):
+    """AUTO with a budget below the full trajectory (131 states): 100 states
+    let the binomial schedule recompute 32 steps against sqrt's 119, so it is
+    taken in both modes; with 30 states binomial recomputes 102, which the
+    exact mode still prefers, while the reference mode (whose binomial
+    reversal also loses the kept k1 and copies a state per step) keeps sqrt.
+    Every choice gives the bits of full storage."""
+    inst = _inst(48, 130, seed=23, ncols=64, objective="gradient")
+    args = (inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows, inst.ghost,
+            inst.gamma, inst.S, 0.2)
+    full = api.fk_grad_Et(*args, params=inst.params,
+                          opts=api.options(grad_mode=mode, ckpt_policy=_lib.CKPT_FULL))
+    sb = _state_bytes(inst.nrows, inst.ncols)
+    for states, want in ((100, "binomial"), (30, "binomial" if mode == _lib.GRAD_EXACT else "sqrt")):
+        opts = api.options(grad_mode=mode, ckpt_policy=_lib.CKPT_AUTO, ckpt_budget_bytes=states * sb)
+        with api.Problem(inst, opts=opts) as pb:
+            r = pb.grad(inst.Et, inst.y0)
+            plan = pb.last_plan
+        assert plan["policy"] == want, (states, plan)
+        assert plan["recompute_steps"] == {"sqrt": 119, "binomial": 32 if states == 100 else 102}[want]
+        assert np.array_equal(r["gradE"], full[0])
+        assert r["Lcost"] == full[1]

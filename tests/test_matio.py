@@ -18,7 +18,9 @@ import scipy.sparse as sp
 from fkadj import matio
 from fkadj._lib import FkadjError
 
-REF_DATA = "/root/reference/src/cuda/data"
+from conftest import reference_dir
+
+REF_DATA = os.path.join(reference_dir() or "", "src", "cuda", "data")
 BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "adjoint-optimization_b200",
                    "bin")
 

@@ -9,8 +9,9 @@ device array inside the library.
 
 With alpha = 0 the reference's gradient ends in gradE[nt] = -z(T).gh, with
 z(T) = -gamma_u S u(T); the entry point applied to that z(T) must return
--gradE[nt].  Each grid is checked on two calls in a row, and two grids of
-different sizes follow each other, so the shared scratch always holds the
+-gradE[nt].  Each grid is checked on two calls in a row, and grids of
+different sizes follow each other (whole and ragged 16x16 sub-block lattices,
+a smaller lattice after a larger one), so the shared scratch always holds the
 previous call's values when a call starts.
 """
 import ctypes as C
@@ -35,7 +36,10 @@ def test_noalloc_zgh_matches_gradient_entry_point():
     import torch
     L, fn = _entry()
     stream = torch.cuda.current_stream()
-    for seed, (nr, nc) in ((71, (64, 80)), (72, (96, 48))):
+    # 64x80 and 96x48 are whole 16x16 sub-blocks; 67x83 and 19x50 end in partial
+    # ones at the right and bottom edges (the kernel's edge guards), and 19x50
+    # (8 sub-blocks) follows 67x83 (30), so its call starts on stale partials
+    for seed, (nr, nc) in ((71, (64, 80)), (72, (96, 48)), (73, (67, 83)), (74, (19, 50))):
         inst = W.make_instance(nr, 60, seed=seed, ncols=nc, n_obstacles=6, objective="gradient")
         gradE, Lc, L0, LE, _, yf = api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index,
                                                   inst.ncols, inst.nrows, inst.ghost, inst.gamma, inst.S, 0.0,
