@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace fkadj {
@@ -45,8 +46,13 @@ BatchEngine::~BatchEngine() {
     cudaFreeHost(t_fwd_);
     cudaFreeHost(t_mid_);
     cudaFreeHost(t_adj_);
+    cudaFreeHost(t_fus_);
     for (auto& e : qev_)
         if (e) cudaEventDestroy(e);
+    for (auto& e : bev_)
+        if (e) cudaEventDestroy(e);
+    for (auto& g : bgraphs_) cudaGraphExecDestroy(g.second);
+    if (bring_) cudaFreeHost(bring_);
     if (qring_) cudaFreeHost(qring_);
     if (own_stream_ && st_) cudaStreamDestroy(st_);
 }
@@ -63,6 +69,17 @@ fkadj_status BatchEngine::init(const fkadj_options* opt) {
     }
     const int t = batch_preset((opt_.tile > 0 && opt_.tile <= tile_count()) ? opt_.tile - 1 : 0);
     tiles_[0] = tiles_[1] = tiles_[2] = t;
+    tiles_[3] = 0;
+    // the split midpoint + step kernels unless the autotuner (or FKADJ_ADJ_PATH) picks the fused step
+    adj_path_ = Problem::ADJ_SPLIT;
+    if (const char* ap = getenv("FKADJ_ADJ_PATH")) {
+        if (!std::strcmp(ap, "fused")) adj_path_ = Problem::ADJ_FUSED;
+        else if (!std::strcmp(ap, "fused-recompute")) adj_path_ = Problem::ADJ_FUSED_RECOMPUTE;
+    }
+    if (const char* ft = getenv("FKADJ_FUSED_TILE")) {
+        const int f = std::atoi(ft);
+        if (f >= 0 && f < fused_count()) tiles_[3] = f;
+    }
     tuned_ = opt_.tile > 0 && opt_.tile <= tile_count();
     hw_ = hermite_weights();
     {
@@ -78,11 +95,21 @@ fkadj_status BatchEngine::init(const fkadj_options* opt) {
         uint64_t keep = UINT64_MAX;
         BCK(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
     }
-    BCK(cudaMallocHost(&qring_, sizeof(BatchItem) * (size_t)kQueueRing * 3 * kBatchMaxItems), "queue ring");
-    BCK(qdev_.alloc(sizeof(BatchItem) * 3 * kBatchMaxItems), "device queue");
+    BCK(cudaMallocHost(&qring_, sizeof(BatchItem) * (size_t)kQueueRing * 4 * kBatchMaxItems), "queue ring");
+    BCK(qdev_.alloc(sizeof(BatchItem) * 4 * kBatchMaxItems), "device queue");
     BCK(cudaMallocHost(&t_fwd_, sizeof(BatchTick)), "pinned tick");
     BCK(cudaMallocHost(&t_mid_, sizeof(BatchTick)), "pinned tick");
     BCK(cudaMallocHost(&t_adj_, sizeof(BatchTick)), "pinned tick");
+    BCK(cudaMallocHost(&t_fus_, sizeof(BatchTick)), "pinned tick");
+    {
+        const char* bg = getenv("FKADJ_BATCH_GRAPHS");
+        block_graphs_ = !(bg && bg[0] == '0') && st_ != nullptr && st_ != cudaStreamLegacy &&
+                        st_ != cudaStreamPerThread;
+    }
+    if (block_graphs_) {
+        BCK(cudaMallocHost(&bring_, block_bytes() * kBlockRing), "pinned block staging");
+        BCK(bdev_.alloc(block_bytes()), "device block");
+    }
     return FKADJ_OK;
 }
 
@@ -107,6 +134,7 @@ fkadj_status BatchEngine::add_problem(const fkadj_params& p, double dt, int nt, 
     bi.g = pb->g_;
     bi.gh = pb->gh_.as<double>();
     bi.wc = pb->wc_.as<uint8_t>();
+    bi.fault = pb->fault();
     bi.nsbx = pb->nsbx_;
     int slot = -1;
     for (size_t k = 0; k < probs_.size(); ++k)
@@ -241,7 +269,7 @@ fkadj_status BatchEngine::submit(int prob, const double* Et, const double* y_ini
         j->cur = P.state_buf(0);
     }
     if ((s = build_plan(*j))) return s;
-    j->h_out = take_pinned((size_t)j->rows + 1, &j->h_cap);
+    j->h_out = take_pinned((size_t)j->rows + 2, &j->h_cap);  // [0] L0 sum, [1..rows], fault word
     if (!j->h_out) {
         set_error("pinned results: out of host memory");
         return FKADJ_ERR_NOMEM;
@@ -284,6 +312,12 @@ fkadj_status BatchEngine::host_action(Job& j, const Action& a) {
             "download");
     }
     BCK(cudaMemcpyAsync(j.h_out, P.osum_.p, sizeof(double), cudaMemcpyDeviceToHost, st_), "download");
+    // the problem's fault word after the job's launches (a tile copy whose
+    // bounded wait expired), then cleared for the problem's next job
+    unsigned* hf = reinterpret_cast<unsigned*>(j.h_out + j.rows + 1);
+    *hf = 0;
+    BCK(cudaMemcpyAsync(hf, P.fault(), sizeof(unsigned), cudaMemcpyDeviceToHost, st_), "download fault word");
+    BCK(cudaMemsetAsync(P.fault(), 0, sizeof(unsigned), st_), "clear fault word");
     BCK(cudaEventRecord(j.ev, st_), "event");
     j.finishing = true;
     return FKADJ_OK;
@@ -298,8 +332,8 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
     // each kernel kind runs its own tile preset: the queue of kind k is cut
     // into tiles of that preset
     auto ntiles = [&](const BatchTick* T, int& ntx) {
-        const int k = T == t_fwd_ ? 0 : (T == t_mid_ ? 1 : 2);
-        const TileShape ts = tile_shape(tiles_[k]);
+        const int k = T == t_fwd_ ? 0 : (T == t_mid_ ? 1 : (T == t_adj_ ? 2 : 3));
+        const TileShape ts = k == 3 ? fused_shape(tiles_[3]) : tile_shape(tiles_[k]);
         ntx = (P.g_.ncols + ts.tx - 1) / ts.tx;
         return ntx * ((P.g_.nrows + ts.ty - 1) / ts.ty);
     };
@@ -367,6 +401,31 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
             const int nxt = 1 - j.cur_c;
             const double* ya = seg(i - 1, k);
             const double* yb = seg(i, k);
+            const double* fa = kept(i - 1, k);
+            const double* fb = kept(i, k);
+            if (adj_path_ != Problem::ADJ_SPLIT) {  // one fused step
+                const bool cache = adj_path_ == Problem::ADJ_FUSED;
+                it.kind = BATCH_ADJ_FUSED;
+                it.a = j.z;
+                it.out = j.z2;
+                it.b = yb;
+                it.d = ya;
+                it.fa = fa;
+                it.fin = fb ? fb : (j.have_fcarry ? fc[j.cur_c] : nullptr);
+                it.fout = fa ? nullptr : fc[nxt];
+                it.E0 = P.Et_[i - 1];
+                it.E1 = P.Et_[i];
+                it.E2 = P.E3_[i - 1];
+                it.row = P.partial_.as<double>() + (size_t)(i - 1) * nsb;
+                it.jb = (cache && j.have_jcarry) ? jy[j.cur_c] : nullptr;
+                it.ja = cache ? jy[nxt] : nullptr;
+                push(t_fus_, it);
+                std::swap(j.z, j.z2);
+                j.cur_c = nxt;
+                j.have_fcarry = fa == nullptr;
+                j.have_jcarry = cache;
+                break;
+            }
             BatchItem m{};
             m.kind = BATCH_MID;
             m.a = ya;
@@ -375,8 +434,6 @@ fkadj_status BatchEngine::tick_action(Job& j, const Action& a) {
             m.E0 = P.Et_[i - 1];
             m.E1 = P.Et_[i];
             m.E2 = P.E3_[i - 1];
-            const double* fa = kept(i - 1, k);
-            const double* fb = kept(i, k);
             m.fa = fa;
             m.fin = fb ? fb : (j.have_fcarry ? fc[j.cur_c] : nullptr);
             m.fout = fa ? nullptr : fc[nxt];
@@ -464,6 +521,11 @@ fkadj_status BatchEngine::finish_poll(Job& j) {
     bool finite = std::isfinite(l0);
     for (size_t i = 0; finite && i < j.gradE.size(); ++i) finite = std::isfinite(j.gradE[i]);
     j.status = finite ? FKADJ_OK : FKADJ_ERR_NUMERIC;
+    if (*reinterpret_cast<const unsigned*>(j.h_out + j.rows + 1)) {
+        set_error("a bounded wait in a batched kernel expired (tile copy into shared memory); the job's results "
+                  "are invalid");
+        j.status = FKADJ_ERR_TIMEOUT;
+    }
     j.done = true;
     j.t_done = host_seconds();
     return FKADJ_OK;
@@ -491,13 +553,15 @@ fkadj_status BatchEngine::tick(int* active) {
             tiles_[1] = batch_preset(P.tk_[Problem::T_MID]);
             tiles_[2] = batch_preset(P.grad_mode_ == FKADJ_GRAD_EXACT ? P.tk_[Problem::T_EXACT]
                                                                        : P.tk_[Problem::T_ADJ]);
+            if (P.grad_mode_ == FKADJ_GRAD_REF && P.forced_path_ < 0) {
+                adj_path_ = P.adj_path_;
+                tiles_[3] = P.tkf_;
+            }
             tuned_ = true;
         }
     }
-    t_fwd_->n = t_fwd_->tiles = 0;
-    t_mid_->n = t_mid_->tiles = 0;
-    t_adj_->n = t_adj_->tiles = 0;
-    std::vector<int> still;
+    // finished jobs and host actions first; `ready` jobs have a device action next
+    std::vector<int> still, ready;
     still.reserve(active_.size());
     for (int id : active_) {
         Job& j = *jobs_[id];
@@ -507,34 +571,67 @@ fkadj_status BatchEngine::tick(int* active) {
             continue;
         }
         while (j.pc < j.plan.size()) {
-            const Action a = j.plan[j.pc++];
-            if (a.kind == Action::OBJ || a.kind == Action::FINISH) {
-                if ((s = host_action(j, a))) return s;
-                if (a.kind == Action::FINISH) break;
-                continue;
-            }
-            if ((s = tick_action(j, a))) return s;
-            break;
+            const Action a = j.plan[j.pc];
+            if (a.kind != Action::OBJ && a.kind != Action::FINISH) break;
+            ++j.pc;
+            if ((s = host_action(j, a))) return s;
+            if (a.kind == Action::FINISH) break;
         }
         still.push_back(id);
+        if (!j.finishing && j.pc < j.plan.size()) ready.push_back(id);
     }
     active_.swap(still);
+    int K = 1;
+    if (block_graphs_ && !ready.empty()) {
+        int m = kBlockMax;
+        for (int id : ready) m = std::min(m, device_run(*jobs_[id]));
+        while (K * 2 <= m) K *= 2;  // a power of two: few distinct graphs
+    }
+    if (K >= 2) {
+        if ((s = launch_block(K, ready))) return s;
+    } else {
+        t_fwd_->n = t_fwd_->tiles = 0;
+        t_mid_->n = t_mid_->tiles = 0;
+        t_adj_->n = t_adj_->tiles = 0;
+        t_fus_->n = t_fus_->tiles = 0;
+        for (int id : ready) {
+            Job& j = *jobs_[id];
+            if ((s = tick_action(j, j.plan[j.pc++]))) return s;
+        }
+        if ((s = launch_tick())) return s;
+        ++ticks_;
+    }
+    if (active) *active = (int)active_.size();
+    return FKADJ_OK;
+}
+
+int BatchEngine::device_run(const Job& j) const {
+    int n = 0;
+    for (size_t k = j.pc; k < j.plan.size() && n < kBlockMax; ++k, ++n) {
+        const int kind = j.plan[k].kind;
+        if (kind == Action::OBJ || kind == Action::FINISH) break;
+    }
+    return n;
+}
+
+// One tick: the four queues, packed into the next pinned ring slot and copied
+// to the device queue in one stream-ordered copy (the previous tick's kernels
+// are done with it by then); a slot is reused kQueueRing ticks later, after
+// its copy's event.
+fkadj_status BatchEngine::launch_tick() {
     const BatchInstance* inst = inst_dev_.as<BatchInstance>();
-    // the three queues, packed into the next pinned ring slot and copied to the
-    // device queue in one stream-ordered copy (the previous tick's kernels are
-    // done with it by then); a slot is reused kQueueRing ticks later, after its
-    // copy's event
-    const int nf = t_fwd_->n, nm = t_mid_->n, na = t_adj_->n;
-    if (nf + nm + na > 0) {
+    const int nf = t_fwd_->n, nm = t_mid_->n, na = t_adj_->n, nu = t_fus_->n;
+    if (nf + nm + na + nu > 0) {
         const int k = (int)(qcount_++ % kQueueRing);
         if (qev_[k]) BCK(cudaEventSynchronize(qev_[k]), "queue slot");
         else BCK(cudaEventCreateWithFlags(&qev_[k], cudaEventDisableTiming), "queue event");
-        BatchItem* slot = qring_ + (size_t)k * 3 * kBatchMaxItems;
+        BatchItem* slot = qring_ + (size_t)k * 4 * kBatchMaxItems;
         std::copy(t_fwd_->item, t_fwd_->item + nf, slot);
         std::copy(t_mid_->item, t_mid_->item + nm, slot + nf);
         std::copy(t_adj_->item, t_adj_->item + na, slot + nf + nm);
+        std::copy(t_fus_->item, t_fus_->item + nu, slot + nf + nm + na);
         BatchItem* dq = qdev_.as<BatchItem>();
-        BCK(cudaMemcpyAsync(dq, slot, sizeof(BatchItem) * (size_t)(nf + nm + na), cudaMemcpyHostToDevice, st_),
+        BCK(cudaMemcpyAsync(dq, slot, sizeof(BatchItem) * (size_t)(nf + nm + na + nu), cudaMemcpyHostToDevice, st_),
             "upload queue");
         BCK(cudaEventRecord(qev_[k], st_), "queue event");
         BCK(launch_batch_fwd(tiles_[0], inst, BatchQueue{dq, nf, t_fwd_->tiles}, st_), "batched forward");
@@ -542,10 +639,94 @@ fkadj_status BatchEngine::tick(int* active) {
             "batched midpoint");
         BCK(launch_batch_adj(tiles_[2], inst, BatchQueue{dq + nf + nm, na, t_adj_->tiles}, st_),
             "batched adjoint");
+        BCK(launch_batch_fused(tiles_[3], inst, BatchQueue{dq + nf + nm + na, nu, t_fus_->tiles}, hw_, st_),
+            "batched fused adjoint");
     }
-    launches_ += (t_fwd_->n > 0) + (t_mid_->n > 0) + (t_adj_->n > 0);
-    ++ticks_;
-    if (active) *active = (int)active_.size();
+    launches_ += (nf > 0) + (nm > 0) + (na > 0) + (nu > 0);
+    return FKADJ_OK;
+}
+
+// K ticks of the ready jobs (each takes its next K actions, all device work):
+// the queues of tick t and kind k are planned into the staging slot, their
+// header (n, tiles, first item) at [t][k]; one copy moves the slot to the
+// device block, and a graph of K ticks x the kinds present replays the
+// launches, each reading its header.  If this stream cannot be captured the
+// same launches are issued directly.
+fkadj_status BatchEngine::launch_block(int K, const std::vector<int>& ready) {
+    const int r = (int)(bcount_++ % kBlockRing);
+    if (bev_[r]) BCK(cudaEventSynchronize(bev_[r]), "block slot");
+    else BCK(cudaEventCreateWithFlags(&bev_[r], cudaEventDisableTiming), "block event");
+    char* slot = bring_ + (size_t)r * block_bytes();
+    int* hdr = reinterpret_cast<int*>(slot);
+    BatchItem* items = reinterpret_cast<BatchItem*>(slot + block_hdr_bytes());
+    BatchTick* T[4] = {t_fwd_, t_mid_, t_adj_, t_fus_};
+    int used = 0, mask = 0;
+    fkadj_status s;
+    for (int t = 0; t < K; ++t) {
+        for (BatchTick* q : T) q->n = q->tiles = 0;
+        for (int id : ready) {
+            Job& j = *jobs_[id];
+            if ((s = tick_action(j, j.plan[j.pc++]))) return s;
+        }
+        for (int k = 0; k < 4; ++k) {
+            int* h = hdr + (t * 4 + k) * 4;
+            h[0] = T[k]->n;
+            h[1] = T[k]->tiles;
+            h[2] = used;
+            h[3] = 0;
+            std::copy(T[k]->item, T[k]->item + T[k]->n, items + used);
+            used += T[k]->n;
+            if (T[k]->n > 0) mask |= 1 << k;
+        }
+    }
+    BCK(cudaMemcpyAsync(bdev_.p, slot, block_hdr_bytes() + sizeof(BatchItem) * (size_t)used, cudaMemcpyHostToDevice,
+                        st_),
+        "upload block");
+    BCK(cudaEventRecord(bev_[r], st_), "block event");
+    const std::pair<int, int> key{K, mask};
+    const BatchInstance* inst = inst_dev_.as<BatchInstance>();
+    const BatchItem* dbase = reinterpret_cast<const BatchItem*>(bdev_.as<char>() + block_hdr_bytes());
+    const int* dhdr = bdev_.as<int>();
+    auto issue = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int t = 0; t < K && e == cudaSuccess; ++t) {
+            auto q = [&](int k) { return BatchQueue{dbase, 0, 0, dhdr + (t * 4 + k) * 4}; };
+            if (!e && (mask & 1)) e = launch_batch_fwd(tiles_[0], inst, q(0), st_);
+            if (!e && (mask & 2)) e = launch_batch_mid(tiles_[1], inst, q(1), hw_, st_);
+            if (!e && (mask & 4)) e = launch_batch_adj(tiles_[2], inst, q(2), st_);
+            if (!e && (mask & 8)) e = launch_batch_fused(tiles_[3], inst, q(3), hw_, st_);
+        }
+        return e;
+    };
+    cudaGraphExec_t gx = nullptr;
+    for (auto& g : bgraphs_)
+        if (g.first == key) gx = g.second;
+    if (!gx) {
+        cudaError_t e = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            set_launch_pdl(false);
+            e = issue();
+            set_launch_pdl(true);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(st_, &graph);
+            if (e == cudaSuccess) e = ec;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&gx, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            gx = nullptr;
+            block_graphs_ = false;
+            BCK(issue(), "block launches");
+            launches_ += (int64_t)K * __builtin_popcount(mask);
+            ticks_ += K;
+            return FKADJ_OK;
+        }
+        bgraphs_.push_back({key, gx});
+    }
+    BCK(cudaGraphLaunch(gx, st_), "block graph");
+    launches_ += (int64_t)K * __builtin_popcount(mask);
+    ticks_ += K;
     return FKADJ_OK;
 }
 

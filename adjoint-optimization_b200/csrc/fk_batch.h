@@ -95,7 +95,8 @@ private:
     cudaStream_t st_ = nullptr;
     bool own_stream_ = false;
     cudaMemPool_t pool_ = nullptr;  // device memory of the engine's problems
-    int tiles_[3] = {0, 0, 0};  // fwd, mid, adj presets
+    int tiles_[4] = {0, 0, 0, 0};  // fwd, mid, adj presets; fused preset (fused_shape)
+    int adj_path_ = 0;             // reference-adjoint path (Problem::AdjPath), from the autotuner
     bool tuned_ = false;        // presets fixed (options.tile > 0) or autotuned
     HermiteW hw_{};
     std::vector<std::unique_ptr<Problem>> probs_;
@@ -105,15 +106,35 @@ private:
     std::vector<std::unique_ptr<Job>> jobs_;
     std::vector<int> active_;  // job ids in tick order
     static constexpr int kQueueRing = 64;
-    BatchItem* qring_ = nullptr;        // pinned: kQueueRing slots of 3 x kBatchMaxItems items
+    BatchItem* qring_ = nullptr;        // pinned: kQueueRing slots of 4 x kBatchMaxItems items
     cudaEvent_t qev_[kQueueRing] = {};  // a slot's copy has run
     uint64_t qcount_ = 0;
     DevBuf qdev_;                       // the device queue the kernels read
-    BatchTick* t_fwd_ = nullptr;  // host staging of the three queues
+    BatchTick* t_fwd_ = nullptr;  // host staging of the four queues
     BatchTick* t_mid_ = nullptr;
     BatchTick* t_adj_ = nullptr;
+    BatchTick* t_fus_ = nullptr;  // fused reference-adjoint steps
     int64_t launches_ = 0, ticks_ = 0;
     fkadj_options opt_{};
+    // Blocks of ticks: while no running job needs host work (its objective or
+    // its results), up to kBlockMax ticks are planned at once, their queues
+    // uploaded in one copy, and their launches replayed from a CUDA graph
+    // captured once per (ticks, kinds present) that reads each queue's size
+    // and place from a header in device memory.  FKADJ_BATCH_GRAPHS=0 keeps
+    // one tick at a time.
+    static constexpr int kBlockMax = 32;
+    static constexpr int kBlockRing = 4;
+    bool block_graphs_ = true;
+    char* bring_ = nullptr;             // pinned staging: kBlockRing slots of block_bytes()
+    cudaEvent_t bev_[kBlockRing] = {};  // a slot's copy has run
+    uint64_t bcount_ = 0;
+    DevBuf bdev_;                       // the device block: headers, then items
+    std::vector<std::pair<std::pair<int, int>, cudaGraphExec_t>> bgraphs_;  // (ticks, kind mask) -> graph
+    static size_t block_hdr_bytes() { return (size_t)kBlockMax * 4 * 4 * sizeof(int); }
+    static size_t block_bytes() { return block_hdr_bytes() + sizeof(BatchItem) * (size_t)kBlockMax * 4 * kBatchMaxItems; }
+    int device_run(const Job& j) const;  // device actions before the job's next host action
+    fkadj_status launch_block(int K, const std::vector<int>& ready);
+    fkadj_status launch_tick();
     // Pinned result buffers, reused across jobs: cudaFreeHost synchronises the
     // device, which would stall every running job each time one finishes.
     std::vector<std::pair<size_t, double*>> pinned_free_;

@@ -50,7 +50,24 @@ struct DevModel {
 struct DevGrid {
     int nrows, ncols, ld, rows_alloc;
     long long plane;  // doubles per field plane
+    // Forward stencil code per padded cell (null: the NaN tests decide).
+    const uint8_t* fcode;
 };
+
+// Forward stencil codes: which neighbour the 5-point Laplacian takes in each
+// direction, fixed by the geometry.  The reference replaces a missing (NaN)
+// neighbour by the opposite one (cu-F:319-420); these bits say so ahead of
+// time, so the stencil reads the right neighbours without testing values:
+//   FC_N  north missing: take the south neighbour for north
+//   FC_S  south missing and north present: take the north neighbour for south
+//   FC_W, FC_E  the same across
+//   FC_HOLE  the cell is a hole or outside the grid (its result is NaN)
+// (with north and south both missing both reads take the south neighbour,
+// NaN, as the reference's rule does).  The codes equal the NaN tests as long
+// as no active cell has two opposite holes: such a cell turns NaN after its
+// first stage and its neighbours then mirror it, which no fixed code
+// describes; problems with such cells keep the NaN tests (fcode null).
+constexpr int FC_N = 1, FC_S = 2, FC_W = 4, FC_E = 8, FC_HOLE = 16;
 
 // 1/x for positive x or x = +inf without the division's branches: the hardware
 // reciprocal estimate (rcp.approx.ftz.f64) refined by two Newton-Raphson
@@ -202,12 +219,39 @@ __device__ __forceinline__ double finite_u(double u) {
 #endif
 }
 
+#ifndef FKADJ_FWD_CODES
+#define FKADJ_FWD_CODES 1
+#endif
+
 // Forward vector field at shared-memory cell q of a region W doubles wide with
 // field planes RN apart: 5-point Laplacian with NaN mirroring + F_ion + E*gh.
+// code: the cell's forward stencil code, or -1 to test the values for NaN.
 template <int W, int RN>
 __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restrict__ Y, int q,
-                                       double Egh, double& fu, double& fv, double& fw) {
+                                       double Egh, double& fu, double& fv, double& fw, int code = -1) {
     const double u = Y[q];
+#if FKADJ_FWD_CODES
+    if (code >= 0) {
+        if (code & FC_HOLE) {  // a hole or the NaN ring: its value is NaN, and so is the result
+            fu = fv = fw = u;
+            return;
+        }
+        const int oa = (code & FC_N) ? W : -W, ob = (code & FC_S) ? -W : W;
+        const int oc = (code & FC_W) ? 1 : -1, od = (code & FC_E) ? -1 : 1;
+        const double v = Y[RN + q], w = Y[2 * RN + q];
+        const double* Yv = Y + RN;
+        const double* Yw = Y + 2 * RN;
+        const double lu = P.cu * ((((Y[q + oa] + Y[q + ob]) + Y[q + oc]) + Y[q + od]) - 4.0 * u);
+        const double lv = P.cv * ((((Yv[q + oa] + Yv[q + ob]) + Yv[q + oc]) + Yv[q + od]) - 4.0 * v);
+        const double lw = P.cw * ((((Yw[q + oa] + Yw[q + ob]) + Yw[q + oc]) + Yw[q + od]) - 4.0 * w);
+        double ud, vd, wd;
+        fk_ion(P, u, v, w, ud, vd, wd);
+        fu = (lu + ud) + Egh;
+        fv = lv + vd;
+        fw = lw + wd;
+        return;
+    }
+#endif
 #if FKADJ_HOLE_BRANCH
     // holes and the NaN ring skip the arithmetic (their result is NaN either way)
     if (isnan(u)) {

@@ -177,7 +177,7 @@ Problem::~Problem() {
     if (pool_) {
         // stream-ordered frees need the stream (the problem's own one is destroyed
         // below): release the buffers first
-        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
+        DevBuf* all[] = {&gh_, &wc_, &fcode_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
                          &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
                          &fcache_, &Ed_};
         for (DevBuf* b : all) b->release();
@@ -205,7 +205,7 @@ Problem::~Problem() {
     delete spline_;
     const auto t3 = clk::now();
     if (verbose_ > 1) {
-        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
+        DevBuf* all[] = {&gh_, &wc_, &fcode_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
                          &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
                          &fcache_, &Ed_};
         size_t bytes = 0;
@@ -305,7 +305,7 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
     }
     for (auto& e : ev_) CK(cudaEventCreate(&e), "cudaEventCreate");
     if (pool_) {
-        DevBuf* all[] = {&gh_, &wc_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
+        DevBuf* all[] = {&gh_, &wc_, &fcode_, &pos_, &Srow_, &Scol_, &Sval_, &yc_, &zc_, &opart_, &osum_, &fault_,
                          &work_, &zbuf_, &yh_, &partial_, &zgh_, &traj_, &seg_, &kf_, &y0res_, &stg_, &jcache_,
                          &fcache_, &Ed_};
         for (DevBuf* b : all) b->st = st_, b->pool = pool_;
@@ -378,12 +378,28 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
                                weight(i, j, 0, 1) << 6);
             pos[a - 1] = (long long)o2;
         }
+    // forward stencil codes (FC_*), unless an active cell has two opposite
+    // holes (then the kernels test values for NaN, as the reference does)
+    std::vector<uint8_t> fcode(pl, (uint8_t)FC_HOLE);
+    bool two_opposite = false;
+    for (int i = 0; i < nrows; ++i)
+        for (int j = 0; j < ncols; ++j) {
+            if (!act(i, j)) continue;
+            const bool mN = !act(i - 1, j), mS = !act(i + 1, j), mW = !act(i, j - 1), mE = !act(i, j + 1);
+            two_opposite = two_opposite || (mN && mS) || (mW && mE);
+            fcode[(size_t)(i + HALO) * g_.ld + (j + HALO)] =
+                (uint8_t)((mN ? FC_N : 0) | ((mS && !mN) ? FC_S : 0) | (mW ? FC_W : 0) | ((mE && !mW) ? FC_E : 0));
+        }
+    const bool use_codes = FKADJ_FWD_CODES && !two_opposite;
     CK(gh_.alloc(pl * sizeof(double)), "alloc gh");
     CK(wc_.alloc(pl), "alloc weights");
+    if (use_codes) CK(fcode_.alloc(pl), "alloc stencil codes");
     CK(pos_.alloc((size_t)n_num * sizeof(long long)), "alloc positions");
     // stream-ordered copies (from pageable memory they return once the data is staged)
     CK(cudaMemcpyAsync(gh_.p, gh.data(), pl * sizeof(double), cudaMemcpyHostToDevice, st_), "upload gh");
     CK(cudaMemcpyAsync(wc_.p, wc.data(), pl, cudaMemcpyHostToDevice, st_), "upload weights");
+    if (use_codes) CK(cudaMemcpyAsync(fcode_.p, fcode.data(), pl, cudaMemcpyHostToDevice, st_), "upload codes");
+    g_.fcode = use_codes ? fcode_.as<uint8_t>() : nullptr;
     CK(cudaMemcpyAsync(pos_.p, pos.data(), (size_t)n_num * sizeof(long long), cudaMemcpyHostToDevice, st_),
        "upload positions");
 

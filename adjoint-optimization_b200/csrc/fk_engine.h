@@ -220,6 +220,7 @@ private:
 
     // device buffers
     DevBuf gh_, wc_, pos_, Srow_, Scol_, Sval_, yc_, zc_, opart_, osum_;
+    DevBuf fcode_;     // forward stencil codes (uint8 per padded cell; unset when the NaN tests decide)
     DevBuf fault_;     // this problem's fault word: set by a step kernel whose bounded wait expired
     unsigned* fault() const { return fault_.as<unsigned>(); }
     DevBuf work_;      // 4 states: two ping-pong, z pair is separate

@@ -128,7 +128,9 @@ __device__ __forceinline__ void load_region(double* __restrict__ dst, const doub
 // tiles in turn (the batched kernels) passes `phase`, its count of bulk
 // transfers so far, the same in every thread: the barrier is initialised at
 // the first transfer only and each later one waits on the next phase's
-// parity (a barrier is not re-initialised while in use).
+// parity (a barrier is not re-initialised while in use).  After an expired
+// wait *phase becomes ~0: the barrier's phase is then unknown, and the CTA's
+// later tiles load with vector loads (their problems' results stay valid).
 template <int RCAP, int WIDTH, int NT, bool BULK>
 __device__ __forceinline__ bool load_windows(double* __restrict__ d0, const double* __restrict__ s0,
                                              double* __restrict__ d1, const double* __restrict__ s1, int ld,
@@ -139,7 +141,7 @@ __device__ __forceinline__ bool load_windows(double* __restrict__ d0, const doub
     const bool aligned = vec_ok && ((reinterpret_cast<uintptr_t>(s0) | reinterpret_cast<uintptr_t>(s1) |
                                      reinterpret_cast<uintptr_t>(s2) | (uintptr_t)ld * 8u | (uintptr_t)plane * 8u) &
                                     15) == 0;
-    if (BULK && FKADJ_BULK_LOAD && aligned) {
+    if (BULK && FKADJ_BULK_LOAD && aligned && !(phase && *phase == ~0u)) {
         __shared__ uint64_t bar;
         const uint32_t k = phase ? *phase : 0u;
         uint32_t b;
@@ -158,7 +160,10 @@ __device__ __forceinline__ bool load_windows(double* __restrict__ d0, const doub
         if (d1) bulk_issue<RCAP, WIDTH, NT>(b, d1, s1, ld, plane, rows);
         if (d2) bulk_issue<RCAP, WIDTH, NT>(b, d2, s2, ld, plane, rows);
         if (phase) ++*phase;
-        if (!bulk_wait_cta(b, fault, 1000000000ull, k & 1u)) return false;
+        if (!bulk_wait_cta(b, fault, 1000000000ull, k & 1u)) {
+            if (phase) *phase = ~0u;
+            return false;
+        }
     } else {
         load_region<RCAP, WIDTH, NT>(d0, s0, ld, plane, vec_ok, rows);
         if (d1) load_region<RCAP, WIDTH, NT>(d1, s1, ld, plane, vec_ok, rows);
@@ -223,7 +228,7 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
                                           const double* __restrict__ y0g, const double* __restrict__ ghs,
                                           int ld, long long plane, double Ev, double cY, double cD,
                                           double* __restrict__ out, double* __restrict__ stage_out, int rows,
-                                          double* __restrict__ k_out = nullptr) {
+                                          double* __restrict__ k_out, const uint8_t* __restrict__ fcs) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E;
     constexpr int IN = TX * TY;
@@ -244,7 +249,7 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
             a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
         }
         double ku, kv, kw;
-        rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw);
+        rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw, fcs ? (int)__ldg(fcs + o) : -1);
         const bool inner = (E == 0) || (r >= HALO && r < HALO + rows && c >= HALO && c < HALO + TX);
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
@@ -293,7 +298,7 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
                                               double* __restrict__ yout, const double* __restrict__ gh, double E0,
                                               double Eh, double E1, double* __restrict__ stages, int tbx, int tby,
                                               int ty, double* __restrict__ k1 = nullptr,
-                                              unsigned* fault = nullptr) {
+                                              unsigned* fault = nullptr, uint32_t* phase = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -305,7 +310,7 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
     if (!load_windows<RH, RW, NT, BULK>(A, yin + off, nullptr, nullptr, g.ld, g.plane, vec_ok, rows + 2 * HALO,
-                                        fault))
+                                        fault, nullptr, nullptr, phase))
         return;
     const double* y0g = yin + off;
     const double* ghs = gh + off;
@@ -314,14 +319,15 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     double* s2 = stages ? stages + off : nullptr;
     double* s3 = stages ? stages + sst + off : nullptr;
     double* s4 = stages ? stages + 2 * sst + off : nullptr;
+    const uint8_t* fcs = g.fcode ? g.fcode + off : nullptr;
     fwd_stage<3, TX, TY, NT, 0>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2,
-                                rows, k1 ? k1 + off : nullptr);
+                                rows, k1 ? k1 + off : nullptr, fcs);
     fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3,
-                                rows);
+                                rows, nullptr, fcs);
     fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4,
-                                rows);
+                                rows, nullptr, fcs);
     fwd_stage<0, TX, TY, NT, 2>(P, B, A, D, y0g, ghs, g.ld, g.plane, E1, 0.0, dt * 1.0 / 6.0, yout + off, nullptr,
-                                rows);
+                                rows, nullptr, fcs);
 }
 
 template <int TX, int TY, int NT>
@@ -375,7 +381,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
                                              const HermiteW& hw, const double* __restrict__ fin,
                                              double* __restrict__ fout, double* __restrict__ jh, int tbx, int tby,
                                              int ty, const double* __restrict__ fa = nullptr,
-                                             unsigned* fault = nullptr) {
+                                             unsigned* fault = nullptr, uint32_t* phase = nullptr) {
     constexpr int H2 = 2;
     constexpr int RW = TX + 2 * H2, RH = TY + 2 * H2, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
@@ -388,7 +394,8 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
     // region origin: logical (i0 - 2, j0 - 2) = padded (i0 + 2, j0 + 2)
     const long long off = (long long)(i0 + HALO - H2) * g.ld + (j0 + HALO - H2);
     const bool vec_ok = ((g.ld | (j0 + HALO - H2)) & 1) == 0;
-    if (!load_windows<RH, RW, NT, BULK>(A, ya + off, B, yb + off, g.ld, g.plane, vec_ok, rows + 2 * H2, fault))
+    if (!load_windows<RH, RW, NT, BULK>(A, ya + off, B, yb + off, g.ld, g.plane, vec_ok, rows + 2 * H2, fault,
+                                        nullptr, nullptr, phase))
         return;
     const double dt = P.dt;
     {
@@ -407,14 +414,14 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
                 a0[1] = __ldg(fa + g.plane + o);
                 a0[2] = __ldg(fa + 2 * g.plane + o);
             } else {
-                rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2]);
+                rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
             }
             if (fin) {
                 a1[0] = __ldg(fin + o);
                 a1[1] = __ldg(fin + g.plane + o);
                 a1[2] = __ldg(fin + 2 * g.plane + o);
             } else {
-                rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2]);
+                rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
             }
             const bool inner = r >= H2 && r < H2 + rows && c >= H2 && c < H2 + TX;
             if (inner && fout) {
@@ -445,7 +452,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
             const int s = r * RW + c;
             const long long o = off + (long long)r * g.ld + c;
             double m2[3], yv[3];
-            rhs_at<RW, RN>(P, C, s, E3 * __ldg(gh + o), m2[0], m2[1], m2[2]);
+            rhs_at<RW, RN>(P, C, s, E3 * __ldg(gh + o), m2[0], m2[1], m2[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
 #pragma unroll
             for (int f = 0; f < 3; ++f) {
                 double* p = yh + o + f * g.plane;
@@ -559,7 +566,7 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
                                               const uint8_t* __restrict__ wc, const double* __restrict__ gh,
                                               double* __restrict__ row, int nsbx, const double* __restrict__ jb,
                                               const double* __restrict__ jh, double* __restrict__ ja, int tbx,
-                                              int tby, unsigned* fault = nullptr) {
+                                              int tby, unsigned* fault = nullptr, uint32_t* phase = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
@@ -568,7 +575,9 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    if (!load_windows<RH, RW, NT, BULK>(A, z + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH, fault)) return;
+    if (!load_windows<RH, RW, NT, BULK>(A, z + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH, fault, nullptr,
+                                        nullptr, phase))
+        return;
     const double dt = P.dt;
     adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb, nullptr);
     adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
@@ -679,13 +688,15 @@ constexpr size_t fused_smem_bytes() {
 }
 
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 1)
-    k_adj_fused(DevModel P, DevGrid g, const double* __restrict__ z, double* __restrict__ zout,
-                const double* __restrict__ ya, const double* __restrict__ yb, const double* __restrict__ fa,
-                const double* __restrict__ fb, double* __restrict__ fout, const uint8_t* __restrict__ wc,
-                const double* __restrict__ gh, EStep E, HermiteW hw, double* __restrict__ row, int nsbx,
-                const double* __restrict__ jb, double* __restrict__ ja, unsigned* fault) {
-    pdl_enter();
+__device__ __forceinline__ void adj_fused_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ z,
+                                               double* __restrict__ zout, const double* __restrict__ ya,
+                                               const double* __restrict__ yb, const double* __restrict__ fa,
+                                               const double* __restrict__ fb, double* __restrict__ fout,
+                                               const uint8_t* __restrict__ wc, const double* __restrict__ gh,
+                                               double Ea, double Eb, double E3, const HermiteW& hw,
+                                               double* __restrict__ row, int nsbx, const double* __restrict__ jb,
+                                               double* __restrict__ ja, int tbx, int tby, unsigned* fault,
+                                               uint32_t* phase = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;  // windows: tile + 4
     constexpr int W3 = TX + 6, RN3 = W3 * (TY + 6);                      // y(1/3): tile + 3
     constexpr int WQ = TX + 4, RNQ = WQ * (TY + 4);                      // quartic part / yh: tile + 2
@@ -696,13 +707,13 @@ __global__ void __launch_bounds__(NT, 1)
     double* Y3 = YB + 3 * RN;
     double* Q = Y3 + 3 * RN3;
     double* D = Q + 3 * RNQ;
-    const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+    const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;  // window origin: logical (i0 - 4, j0 - 4)
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    if (!load_windows<RH, RW, NT, true>(Zw, z + off, YA, ya + off, g.ld, g.plane, vec_ok, RH, fault, YB, yb + off))
+    if (!load_windows<RH, RW, NT, true>(Zw, z + off, YA, ya + off, g.ld, g.plane, vec_ok, RH, fault, YB, yb + off,
+                                        phase))
         return;
     const double dt = P.dt;
-    const double Ea = E.a(), Eb = E.b(), E3 = E.c();
     // y(1/3) (cubic Hermite) on the tile + 3 and the quartic part of yh on the tile + 2
     {
         constexpr int W = TX + 6;
@@ -720,14 +731,14 @@ __global__ void __launch_bounds__(NT, 1)
                 a0[1] = __ldg(fa + g.plane + o);
                 a0[2] = __ldg(fa + 2 * g.plane + o);
             } else {
-                rhs_at<RW, RN>(P, YA, s, Ea * gg, a0[0], a0[1], a0[2]);
+                rhs_at<RW, RN>(P, YA, s, Ea * gg, a0[0], a0[1], a0[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
             }
             if (fb) {
                 a1[0] = __ldg(fb + o);
                 a1[1] = __ldg(fb + g.plane + o);
                 a1[2] = __ldg(fb + 2 * g.plane + o);
             } else {
-                rhs_at<RW, RN>(P, YB, s, Eb * gg, a1[0], a1[1], a1[2]);
+                rhs_at<RW, RN>(P, YB, s, Eb * gg, a1[0], a1[1], a1[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
             }
             if (fout && r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX) {
                 fout[o] = a0[0];
@@ -759,7 +770,8 @@ __global__ void __launch_bounds__(NT, 1)
             const int s3 = (r - 1) * W3 + (c - 1);
             const int sq = (r - 2) * WQ + (c - 2);
             double m2[3];
-            rhs_at<W3, RN3>(P, Y3, s3, E3 * __ldg(gh + o), m2[0], m2[1], m2[2]);
+            rhs_at<W3, RN3>(P, Y3, s3, E3 * __ldg(gh + o), m2[0], m2[1], m2[2],
+                            g.fcode ? (int)__ldg(g.fcode + o) : -1);
 #pragma unroll
             for (int f = 0; f < 3; ++f) Q[f * RNQ + sq] = Q[f * RNQ + sq] + hw.c2 * (m2[f] * dt);
         }
@@ -786,6 +798,18 @@ __global__ void __launch_bounds__(NT, 1)
     fused_stage<0, TX, TY, NT, 2>(P, g, YB, YA, D, Zw, wc, off, 0.0, 1.0 / 6.0 * dt, zout, gh, j_ya);
     __syncthreads();
     subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    k_adj_fused(DevModel P, DevGrid g, const double* __restrict__ z, double* __restrict__ zout,
+                const double* __restrict__ ya, const double* __restrict__ yb, const double* __restrict__ fa,
+                const double* __restrict__ fb, double* __restrict__ fout, const uint8_t* __restrict__ wc,
+                const double* __restrict__ gh, EStep E, HermiteW hw, double* __restrict__ row, int nsbx,
+                const double* __restrict__ jb, double* __restrict__ ja, unsigned* fault) {
+    pdl_enter();
+    adj_fused_tile<TX, TY, NT>(P, g, z, zout, ya, yb, fa, fb, fout, wc, gh, E.a(), E.b(), E.c(), hw, row, nsbx, jb,
+                               ja, blockIdx.x, blockIdx.y, fault);
 }
 
 // ------------------------------------------------------ exact-mode adjoint
@@ -864,7 +888,7 @@ __device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid&
                                                const double* __restrict__ stages, const uint8_t* __restrict__ wc,
                                                const double* __restrict__ gh, double* __restrict__ r1,
                                                double* __restrict__ r23, double* __restrict__ r4, int nsbx, int tbx,
-                                               int tby, unsigned* fault = nullptr) {
+                                               int tby, unsigned* fault = nullptr, uint32_t* phase = nullptr) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int IN = TX * TY;
     extern __shared__ double4 smem_raw[];
@@ -875,7 +899,9 @@ __device__ __forceinline__ void adj_exact_tile(const DevModel& P, const DevGrid&
     const int i0 = tby * TY, j0 = tbx * TX;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    if (!load_windows<RH, RW, NT, BULK>(A, lam + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH, fault)) return;
+    if (!load_windows<RH, RW, NT, BULK>(A, lam + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH, fault, nullptr,
+                                        nullptr, phase))
+        return;
     const double dt = P.dt;
     const double c6 = dt / 6.0, c3 = dt / 3.0, c2 = dt * 0.5;
 #pragma unroll 2
@@ -924,27 +950,47 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
 // (one small copy per tick; kernel parameters stay a few bytes); a persistent
 // grid of CTAs strides over the queue's tiles, each item owning a contiguous
 // range of tile indices.
-__device__ __forceinline__ int find_item(const BatchQueue& q, int tile) {
-    int lo = 0, hi = q.n - 1;
+__device__ __forceinline__ int find_item(const BatchItem* items, int n, int tile) {
+    int lo = 0, hi = n - 1;
     while (lo < hi) {  // last item whose first tile is <= tile
         const int mid = (lo + hi + 1) >> 1;
-        if (q.items[mid].tile0 <= tile) lo = mid;
+        if (items[mid].tile0 <= tile) lo = mid;
         else hi = mid - 1;
     }
     return lo;
 }
 
+// The queue a batched launch works on: by value, or from its device header.
+struct QueueView {
+    const BatchItem* items;
+    int n, tiles;
+    __device__ __forceinline__ explicit QueueView(const BatchQueue& q) {
+        if (q.hdr) {
+            n = q.hdr[0];
+            tiles = q.hdr[1];
+            items = q.items + q.hdr[2];
+        } else {
+            n = q.n;
+            tiles = q.tiles;
+            items = q.items;
+        }
+    }
+    __device__ __forceinline__ const BatchItem& item(int tile) const { return items[find_item(items, n, tile)]; }
+};
+
 template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
-    for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
-        const BatchItem& it = t.items[find_item(t, tile)];
+    uint32_t phase = 0;  // bulk transfers of this CTA so far (the tile-copy barrier's phase)
+    const QueueView q(t);
+    for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {
+        const BatchItem& it = q.item(tile);
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
-        fwd_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, I.gh, it.E0, it.E1, it.E2, it.stages, tbx, tby, TY,
-                                  it.k1);
+        fwd_step_tile<TX, TY, NT, true>(I.P, I.g, it.a, it.out, I.gh, it.E0, it.E1, it.E2, it.stages, tbx, tby, TY,
+                                        it.k1, I.fault, &phase);
     }
 }
 
@@ -952,13 +998,15 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_mid(const BatchInstance* __restrict__ inst, const BatchQueue t, HermiteW hw) {
     pdl_enter();
-    for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
-        const BatchItem& it = t.items[find_item(t, tile)];
+    uint32_t phase = 0;
+    const QueueView q(t);
+    for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {
+        const BatchItem& it = q.item(tile);
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
-        adj_mid_tile<TX, TY, NT>(I.P, I.g, it.a, it.b, I.gh, it.out, it.E0, it.E1, it.E2, hw, it.fin, it.fout,
-                                 it.jh, tbx, tby, TY, it.fa);
+        adj_mid_tile<TX, TY, NT, true>(I.P, I.g, it.a, it.b, I.gh, it.out, it.E0, it.E1, it.E2, hw, it.fin, it.fout,
+                                       it.jh, tbx, tby, TY, it.fa, I.fault, &phase);
     }
 }
 
@@ -966,17 +1014,35 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_adj(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
-    for (int tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
-        const BatchItem& it = t.items[find_item(t, tile)];
+    uint32_t phase = 0;
+    const QueueView q(t);
+    for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {
+        const BatchItem& it = q.item(tile);
         const BatchInstance& I = inst[it.inst];
         const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
         __syncthreads();
         if (it.kind == BATCH_ADJ_EXACT)
-            adj_exact_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, it.b, it.stages, I.wc, I.gh, it.row, it.row2,
-                                       it.row3, I.nsbx, tbx, tby);
+            adj_exact_tile<TX, TY, NT, true>(I.P, I.g, it.a, it.out, it.b, it.stages, I.wc, I.gh, it.row, it.row2,
+                                             it.row3, I.nsbx, tbx, tby, I.fault, &phase);
         else
-            adj_step_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, it.b, it.c, it.d, I.wc, I.gh, it.row, I.nsbx, it.jb,
-                                      it.jh, it.ja, tbx, tby);
+            adj_step_tile<TX, TY, NT, true>(I.P, I.g, it.a, it.out, it.b, it.c, it.d, I.wc, I.gh, it.row, I.nsbx,
+                                            it.jb, it.jh, it.ja, tbx, tby, I.fault, &phase);
+    }
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, 1) k_batch_fused(const BatchInstance* __restrict__ inst, const BatchQueue t,
+                                                       HermiteW hw) {
+    pdl_enter();
+    uint32_t phase = 0;
+    const QueueView q(t);
+    for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {
+        const BatchItem& it = q.item(tile);
+        const BatchInstance& I = inst[it.inst];
+        const int local = tile - it.tile0, tbx = local % it.ntx, tby = local / it.ntx;
+        __syncthreads();
+        adj_fused_tile<TX, TY, NT>(I.P, I.g, it.a, it.out, it.d, it.b, it.fa, it.fin, it.fout, I.wc, I.gh, it.E0,
+                                   it.E1, it.E2, hw, it.row, I.nsbx, it.jb, it.ja, tbx, tby, I.fault, &phase);
     }
 }
 
@@ -1200,6 +1266,9 @@ cudaError_t kernels_init() {
 #define X(id, a, b, c)                                                                                  \
     if ((e = cudaFuncSetAttribute(k_adj_fused<a, b, c>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                   (int)fused_smem_bytes<a, b>())) != cudaSuccess)                        \
+        return e;                                                                                        \
+    if ((e = cudaFuncSetAttribute(k_batch_fused<a, b, c>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)fused_smem_bytes<a, b>())) != cudaSuccess)                        \
         return e;
     FKADJ_FUSED_LIST(X)
 #undef X
@@ -1349,11 +1418,15 @@ cudaError_t launch_adj_fused(int tile, const DevModel& P, const DevGrid& g, cons
     return cudaGetLastError();
 }
 
+// A launch whose queue is read from its device header (t.hdr) takes the full
+// persistent grid: the number of tiles is not known on the host.
+static int queue_tiles(const BatchQueue& t) { return t.hdr ? (1 << 30) : t.tiles; }
+
 cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchQueue& t, cudaStream_t st) {
-    if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
+    if (!t.hdr && (t.n <= 0 || t.tiles <= 0)) return cudaSuccess;
     DISPATCH(tile, {
         const size_t sm = stencil_smem<TX, TY>(NT);
-        const int grid = persistent_grid(k_batch_fwd<TX, TY, NT>, NT, sm, t.tiles);
+        const int grid = persistent_grid(k_batch_fwd<TX, TY, NT>, NT, sm, queue_tiles(t));
         const cudaError_t e = launch_pdl(k_batch_fwd<TX, TY, NT>, dim3(grid), NT, sm, st, d_inst, t);
         if (e != cudaSuccess) return e;
     });
@@ -1362,10 +1435,10 @@ cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchQ
 
 cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchQueue& t, const HermiteW& hw,
                              cudaStream_t st) {
-    if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
+    if (!t.hdr && (t.n <= 0 || t.tiles <= 0)) return cudaSuccess;
     DISPATCH(tile, {
         const size_t sm = mid_smem<TX, TY>();
-        const int grid = persistent_grid(k_batch_mid<TX, TY, NT>, NT, sm, t.tiles);
+        const int grid = persistent_grid(k_batch_mid<TX, TY, NT>, NT, sm, queue_tiles(t));
         const cudaError_t e = launch_pdl(k_batch_mid<TX, TY, NT>, dim3(grid), NT, sm, st, d_inst, t, hw);
         if (e != cudaSuccess) return e;
     });
@@ -1373,13 +1446,31 @@ cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchQ
 }
 
 cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchQueue& t, cudaStream_t st) {
-    if (t.n <= 0 || t.tiles <= 0) return cudaSuccess;
+    if (!t.hdr && (t.n <= 0 || t.tiles <= 0)) return cudaSuccess;
     DISPATCH(tile, {
         const size_t sm = exact_smem<TX, TY>();
-        const int grid = persistent_grid(k_batch_adj<TX, TY, NT>, NT, sm, t.tiles);
+        const int grid = persistent_grid(k_batch_adj<TX, TY, NT>, NT, sm, queue_tiles(t));
         const cudaError_t e = launch_pdl(k_batch_adj<TX, TY, NT>, dim3(grid), NT, sm, st, d_inst, t);
         if (e != cudaSuccess) return e;
     });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_fused(int tile, const BatchInstance* d_inst, const BatchQueue& t, const HermiteW& hw,
+                               cudaStream_t st) {
+    if (!t.hdr && (t.n <= 0 || t.tiles <= 0)) return cudaSuccess;
+    switch (tile) {
+#define X(id, a, b, c)                                                                                  \
+    case id: {                                                                                          \
+        const size_t sm = fused_smem_bytes<a, b>();                                                      \
+        const int grid = persistent_grid(k_batch_fused<a, b, c>, c, sm, queue_tiles(t));                 \
+        const cudaError_t e = launch_pdl(k_batch_fused<a, b, c>, dim3(grid), c, sm, st, d_inst, t, hw); \
+        if (e != cudaSuccess) return e;                                                                 \
+    } break;
+        FKADJ_FUSED_LIST(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -26,10 +26,11 @@ struct BatchInstance {
     DevGrid g;
     const double* gh;
     const uint8_t* wc;
+    unsigned* fault;  // the problem's fault word (set when a tile copy's bounded wait expires)
     int nsbx;
 };
 
-enum BatchKind { BATCH_FWD = 0, BATCH_MID = 1, BATCH_ADJ_REF = 2, BATCH_ADJ_EXACT = 3 };
+enum BatchKind { BATCH_FWD = 0, BATCH_MID = 1, BATCH_ADJ_REF = 2, BATCH_ADJ_EXACT = 3, BATCH_ADJ_FUSED = 4 };
 
 // One instance's work of one kind in one tick; it owns tiles
 // [tile0, tile0 + ntx*nty) of the tick's launch.  Field use by kind:
@@ -38,6 +39,8 @@ enum BatchKind { BATCH_FWD = 0, BATCH_MID = 1, BATCH_ADJ_REF = 2, BATCH_ADJ_EXAC
 //              fin/fout (f carry), jh (J(yh) out)
 //   ADJ_REF    a = z, out = z_out, b = y_i, c = yh, d = y_{i-1}, row, jb/jh/ja (J caches)
 //   ADJ_EXACT  a = lambda, out = lambda_out, b = y_s, stages, row/row2/row3
+//   ADJ_FUSED  a = z, out = z_out, b = y_i, d = y_{i-1}, fa, fin (f(y_i)), fout, row, jb/ja,
+//              E0/E1/E2 = Et[i-1], Et[i], E(t_{i-1}+dt/3)
 // The three E samples of one step: (E0, Eh, E1) = (Et[i], E(t_i + dt/2),
 // Et[i+1]) for the forward step, (Ea, Eb, E3) = (Et[i-1], Et[i], E(t_{i-1} +
 // dt/3)) for the adjoint midpoint.  Either by value, or read by the kernel from
@@ -79,17 +82,24 @@ struct BatchTick {
 };
 
 // A tick's work queue of one kernel kind as the kernels read it: n items in
-// device memory, `tiles` tiles in all.
+// device memory, `tiles` tiles in all.  With hdr non-null the three numbers
+// are read from device memory instead (hdr[0] = n, hdr[1] = tiles, the items
+// at items + hdr[2]): a launch captured in a CUDA graph then serves any queue
+// written there before it runs.
 struct BatchQueue {
     const BatchItem* items;
     int n;
     int tiles;
+    const int* hdr = nullptr;
 };
 
 cudaError_t launch_batch_fwd(int tile, const BatchInstance* d_inst, const BatchQueue& q, cudaStream_t st);
 cudaError_t launch_batch_mid(int tile, const BatchInstance* d_inst, const BatchQueue& q, const HermiteW& hw,
                              cudaStream_t st);
 cudaError_t launch_batch_adj(int tile, const BatchInstance* d_inst, const BatchQueue& q, cudaStream_t st);
+// fused reference-adjoint steps of a tick; tile: a fused preset (fused_shape)
+cudaError_t launch_batch_fused(int tile, const BatchInstance* d_inst, const BatchQueue& q, const HermiteW& hw,
+                               cudaStream_t st);
 
 int tile_count();
 // The preset the batched kernels run for an autotuned single-instance preset.

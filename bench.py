@@ -57,6 +57,10 @@ BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
 # 126 MB L2.
 FWD_TRAFFIC_PER_CELL = 8656640 / 262144
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
+# fused reference-adjoint step (midpoint + four stages in one launch): read z, y_{i-1}, y_i (72) + kept f(y_{i-1}),
+# f(y_i) (48) + gh (8) + weight and stencil codes (2), write z (24); with the J_F(y)^T cache also read J(y_i) and
+# write J(y_{i-1}) (56 each)
+FUSED_BYTES_PER_CELL = {"fused": 266.0, "fused-recompute": 154.0}
 # discrete-exact adjoint step (--mode exact): read lambda (24), y (24), the three stage states (72), gh (8),
 # weight code (1); write lambda (24)
 EXACT_BYTES_PER_CELL = 153.0
@@ -334,6 +338,10 @@ def run_ours(args):
         names[2], nbytes[2] = "k_adj_exact", EXACT_BYTES_PER_CELL
     else:
         per_grad = {0: inst.nt + recompute, 1: inst.nt, 2: inst.nt}
+        adj = pb.adjoint_kernel
+        if adj["path"] != "split":  # one fused launch per backward step: no midpoint kernel
+            per_grad = {0: inst.nt + recompute, 2: inst.nt}
+            names[2], nbytes[2] = "k_adj_fused", FUSED_BYTES_PER_CELL[adj["path"]]
     kt = {k: pb.kernel_time(k) for k in per_grad}
     tiles = pb.tiles
     share = {k: kt[k][0] * per_grad[k] for k in kt}
@@ -355,6 +363,7 @@ def run_ours(args):
             "time_share": {names[k]: share[k] / sum(share.values()) for k in share},
             "tiles": {k: list(v) for k, v in tiles.items()
                       if (k == "adj_exact") == (args.mode == "exact") or k == "fwd_step"},
+            "adjoint_path": pb.adjoint_kernel,
             "note": "FP64 bound: a vector-field evaluation costs 2 exp, 4 reciprocals and ~60 "
                     "FMA-class operations, 4.6 evaluations per cell-step; the HBM fraction is reported "
                     "against the copy peak"}

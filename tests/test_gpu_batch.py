@@ -74,3 +74,37 @@ def test_objective_only_jobs_and_resident_initial_state():
     ref = api.Problem(inst).objective(inst.Et, inst.y0)
     assert r1["Lcost"] == r2["Lcost"]
     assert abs(r1["Lcost"] - ref["Lcost"]) <= 1e-12 * abs(ref["Lcost"])
+
+
+@pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
+def test_tick_blocks_replayed_as_graphs_give_the_bits_of_single_ticks(monkeypatch, mode):
+    """Runs of ticks without host work are planned together and replayed from
+    a CUDA graph whose launches read their queues from device headers; the
+    results are the bits of one tick at a time (FKADJ_BATCH_GRAPHS=0)."""
+    insts = _mixed(4)
+    out = {}
+    for graphs in ("0", "1"):
+        monkeypatch.setenv("FKADJ_BATCH_GRAPHS", graphs)
+        with Batch() as b:
+            pids = [b.add_problem(i, grad_mode=mode, ckpt_policy=_lib.CKPT_SQRT) for i in insts]
+            jobs = [b.submit(p, i.Et, i.y0) for p, i in zip(pids, insts)]
+            b.run()
+            out[graphs] = ([b.result(j) for j in jobs], b.stats)
+    assert out["1"][1]["ticks"] > 0 and out["0"][1]["ticks"] > 0
+    for a, c in zip(out["0"][0], out["1"][0]):
+        assert np.array_equal(a["gradE"], c["gradE"]) and a["Lcost"] == c["Lcost"]
+
+
+@pytest.mark.parametrize("path", ["fused", "fused-recompute"])
+def test_batched_fused_adjoint_step_matches_the_split_kernels(monkeypatch, path):
+    insts = _mixed(5)
+    out = {}
+    for p in ("split", path):
+        monkeypatch.setenv("FKADJ_ADJ_PATH", p)
+        with Batch() as b:
+            pids = [b.add_problem(i, ckpt_policy=_lib.CKPT_SQRT) for i in insts]
+            jobs = [b.submit(q, i.Et, i.y0) for q, i in zip(pids, insts)]
+            b.run()
+            out[p] = [b.result(j) for j in jobs]
+    for a, c in zip(out["split"], out[path]):
+        assert np.linalg.norm(c["gradE"] - a["gradE"]) <= 1e-13 * np.linalg.norm(a["gradE"])

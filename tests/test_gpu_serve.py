@@ -85,3 +85,25 @@ def test_wait_is_bounded():
         assert done in (True, False)
         assert srv.wait(rid, 120)
         srv.result(rid)
+
+
+def test_served_request_of_each_size_class_matches_the_oracle():
+    """One request of each grid side of the served mix (128 .. 1024), submitted
+    together so they share the batched launches, against the CPU oracle (a
+    short horizon keeps the oracle's 1024^2 run to seconds): Lcost 1e-10 and
+    gradE 1e-8 relative."""
+    import oracle as O
+    sides = (128, 256, 384, 512, 768, 1024)
+    insts = [W.make_instance(n, 24, seed=500 + n, n_obstacles=max(1, round(3e-4 * n * n)), intervals=6,
+                             wavefronts=4, objective="gradient", alpha=0.1) for n in sides]
+    with Server() as srv:
+        ids = [srv.submit(inst) for inst in insts]
+        res = []
+        for rid in ids:
+            assert srv.wait(rid, 300)
+            res.append(srv.result(rid))
+    for inst, r in zip(insts, res):
+        o = O.grad(inst.params, inst.dt, inst.Et, inst.nt, inst.nrows, inst.ncols, inst.y0_grid, inst.gh_grid,
+                   inst.active_index, O.Objective(inst.S, inst.gamma), inst.alpha, mode="ref")
+        assert abs(r["Lcost"] - o["Lcost"]) <= 1e-10 * abs(o["Lcost"]), inst.nrows
+        assert np.linalg.norm(r["gradE"] - o["gradE"]) <= 1e-8 * np.linalg.norm(o["gradE"]), inst.nrows
