@@ -964,8 +964,20 @@ fkadj_status Problem::autotune_trials() {
             });
         // the fused step against the split pair: every preset, with the J(y)
         // cache and re-evaluating J(y); trial launches with kept f, as in the
-        // sqrt sweep
-        const float split_ms = best_ms[T_MID] + best_ms[T_ADJ];
+        // sqrt sweep.  The pair is timed as it runs, midpoint and step launched
+        // in turn (timed one kernel at a time they looked as fast as the fused
+        // step, which ran 6 us slower per backward step in the replayed graph).
+        float split_ms = 0;
+        if (!e)
+            e = timed([&]() {
+                cudaError_t r = launch_adj_mid(tk_[T_MID], P_, g_, y, y, gh_.as<double>(), yh_.as<double>(),
+                                               EStep::values(E, E, E), hw_, st_, fault(), fc, fc + 3 * pl,
+                                               jc + 14 * pl, ty_[T_MID]);
+                if (r) return r;
+                return launch_adj_step(tk_[T_ADJ], P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
+                                       partial_.as<double>(), nsbx_, st_, fault(), jc, jc + 14 * pl, jc + 7 * pl);
+            }, &split_ms);
+        launches_ += 20;
         float fused_best = 1e30f;
         int fused_t = tkf_, fused_p = ADJ_FUSED;
         const bool try_fused = forced_path_ != ADJ_SPLIT;

@@ -680,7 +680,7 @@ __device__ __forceinline__ void fused_stage(const DevModel& P, const DevGrid& g,
 
 // Shared memory of k_adj_fused: windows of z, y_{i-1}, y_i on the tile + 4,
 // y(1/3) on the tile + 3, the quartic part of yh (then yh) on the tile + 2,
-// and the stage accumulator (206 KB at 32x32, 219 KB at 64x16).
+// and the stage accumulator (206 KB at 32x32, 219 KB at 64x16, 119 KB at 32x16).
 template <int TX, int TY>
 constexpr size_t fused_smem_bytes() {
     return sizeof(double) * (9 * (TX + 2 * HALO) * (TY + 2 * HALO) + 3 * (TX + 6) * (TY + 6) +
@@ -1237,13 +1237,14 @@ cudaError_t take_device_fault(cudaStream_t st, unsigned* d_fault, unsigned* faul
     return e;
 }
 
-// Tile presets of the fused reference adjoint (TX, TY, threads): one CTA per
-// SM (its shared memory), TY a multiple of 16 (the z.gh sub-block sums).
+// Tile presets of the fused reference adjoint (TX, TY, threads): TX divides
+// 64 (the padding of a state row: wider tiles would run past the row), TY a
+// multiple of 16 that divides 64 (the z.gh sub-block sums, the row padding).
 #define FKADJ_FUSED_LIST(X) \
     X(0, 32, 32, 512)       \
     X(1, 64, 16, 512)       \
     X(2, 32, 32, 384)       \
-    X(3, 48, 16, 384)
+    X(3, 32, 16, 256)
 
 int fused_count() { return 4; }
 

@@ -14,11 +14,13 @@ wavefronts (large_instance), it measures against T:
                  here (oracle/_ref): the same two differences, which is what
                  the parity tests bound (states 1e-10, gradients 1e-8).
 
-The reference's gradient keeps the whole trajectory in host memory (8 * 3n
-bytes per step), so its horizons are capped (--ref-grad-cap).  One JSON line
-per instance on stdout.
+The reference's gradient keeps the whole trajectory in host memory and
+addresses it with a 32-bit int offset, (i+1)*3*n doubles
+(src/cuda/fk_grad_Et_mono_PARAMETERS.cu:1720 and :1871), which overflows past
+2729 steps at 512^2: its horizons are capped (--ref-grad-cap, 2500).  One JSON
+line per instance goes to --out (the reference's routines print to stdout).
 
-    python tests/chaos_horizon.py [--which c1,c2] [--c2-steps 20000]
+    python tests/chaos_horizon.py [--which c1,c2] [--c2-steps 20000] [--out FILE]
 """
 from __future__ import annotations
 
@@ -38,6 +40,9 @@ for p in (os.path.join(ROOT, "adjoint-optimization_b200"), os.path.join(ROOT, "o
 
 import refbin  # noqa: E402
 from fkadj import api, workloads as W  # noqa: E402
+
+
+OUT = "chaos_horizon.jsonl"
 
 
 def rel_state(a, b):
@@ -122,7 +127,8 @@ def measure(name, inst, nt, nstep, grad_ts, ref_grad_cap, seed=11):
            "grad_horizon_1e-8_vs_reference": horizon([t for t, _ in rg], [e for _, e in rg], 1e-8),
            "state_horizon_1e-10_perturbed": horizon(ts, pert_state, 1e-10),
            "grad_horizon_1e-8_perturbed": horizon(gts, pert_grad, 1e-8)}
-    print(json.dumps(out), flush=True)
+    with open(OUT, "a") as f:
+        f.write(json.dumps(out) + "\n")
     return out
 
 
@@ -130,9 +136,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--which", default="c1,c2")
     ap.add_argument("--c2-steps", type=int, default=20000)
-    ap.add_argument("--ref-grad-cap", type=int, default=4000,
-                    help="longest horizon of the reference binary's gradient at 512^2 (host trajectory memory)")
+    ap.add_argument("--ref-grad-cap", type=int, default=2500,
+                    help="longest horizon of the reference binary's gradient at 512^2 (its int trajectory offset)")
+    ap.add_argument("--out", default="chaos_horizon.jsonl")
     a = ap.parse_args()
+    global OUT
+    OUT = a.out
     which = a.which.split(",")
     if "c1" in which:
         inst = W.plain_instance()
@@ -141,7 +150,7 @@ def main():
         inst = W.large_instance()
         nt = min(a.c2_steps, inst.nt)
         measure("large_instance 512^2", inst, nt, 500,
-                [250, 500, 1000, 2000, 3000, 4000, 6000, 8000, 12000, 16000, 20000], a.ref_grad_cap)
+                [250, 500, 1000, 1500, 2000, 2500, 3000, 4000, 6000, 8000, 12000, 16000, 20000], a.ref_grad_cap)
 
 
 if __name__ == "__main__":
