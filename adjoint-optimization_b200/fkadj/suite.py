@@ -7,11 +7,14 @@
       uneven instances (sides {128..1024}, horizons U{1000..20000} x nt-scale,
       hole density 3e-4, 100-400 intervals): one resident problem at a time vs
       all of them in one batch; gradients/s and makespan
-  python -m fkadj.suite serve  [--rates 10,50,200,500 --requests 48 ...]
+  python -m fkadj.suite serve  [--rates 10,50,200,500 --requests 48 --all-gradients ...]
       Poisson arrivals, half objective-only, half objective+gradient, sizes as
       above: served latency p50/p99 and throughput, against the same stream
       solved one request at a time (FIFO): as plain solves of new instances
-      (set-up included) and as warm resident calls
+      (set-up included) and as warm resident calls.  With --all-gradients and
+      --rates inf it runs the 64-instance batched workload through the server,
+      whose admission by device footprint lets it hold more instances than
+      fit the GPU at once
 
   python -m fkadj.suite opt   [--n 2048 --nt 100000 --iters 1 --probes 4 --budget-gb 60]
       the optimisation loop at scale: Armijo descent on the interval
@@ -158,19 +161,25 @@ def serve_measure(base, grads, rates, rng):
     return out
 
 
-def serve_requests(requests, seed, max_side, nt_scale):
+def serve_requests(requests, seed, max_side, nt_scale, all_gradients=False):
     """The request mix of the served stream: sizes and horizons as the uneven
-    batch (fkadj.workloads.batch_instances), half of them objective+gradient."""
+    batch (fkadj.workloads.batch_instances), half of them objective+gradient
+    (all of them with all_gradients: the batched workload as a request stream)."""
     rng = np.random.default_rng(seed)
     base = _batch_insts(argparse.Namespace(count=requests, seed=seed, max_side=max_side, nt_scale=nt_scale))
     grads = [bool(x) for x in rng.integers(0, 2, size=requests)]
+    if all_gradients:
+        grads = [True] * requests
     return base, grads, rng
 
 
 def cmd_serve(a):
-    base, grads, rng = serve_requests(a.requests, a.seed, a.max_side, a.nt_scale)
+    base, grads, rng = serve_requests(a.requests, a.seed, a.max_side, a.nt_scale, a.all_gradients)
     for r in serve_measure(base, grads, a.rates, rng):
-        r.update({"suite": "serve", "max_side": a.max_side, "nt_scale": a.nt_scale})
+        r.update({"suite": "serve", "max_side": a.max_side, "nt_scale": a.nt_scale,
+                  "all_gradients": a.all_gradients, "sides": sorted({i.nrows for i in base}),
+                  "nt_range": [min(i.nt for i in base), max(i.nt for i in base)],
+                  "gradients": int(sum(grads))})
         print(json.dumps(r), flush=True)
 
 
@@ -207,7 +216,10 @@ def main(argv=None):
             p.add_argument("--nt", type=int, default=2000, help="uniform batch: steps")
         else:
             p.add_argument("--requests", type=int, default=48)
-            p.add_argument("--rates", type=lambda s: [float(x) for x in s.split(",")], default=[10, 50, 200, 500])
+            p.add_argument("--rates", type=lambda s: [float(x) for x in s.split(",")], default=[10, 50, 200, 500],
+                           help="Poisson arrival rates in req/s; inf = every request at once")
+            p.add_argument("--all-gradients", action="store_true",
+                           help="every request objective+gradient (the batched workload as a stream)")
     o = sub.add_parser("opt")
     o.add_argument("--n", type=int, default=2048)
     o.add_argument("--nt", type=int, default=100000)
