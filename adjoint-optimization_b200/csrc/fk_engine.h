@@ -154,7 +154,8 @@ private:
     // Resolves the checkpoint policy.  AUTO takes FULL when the budget holds
     // every state, else whichever of SQRT and BINOMIAL fits and recomputes
     // fewer forward steps (costed in forward-step equivalents, the binomial
-    // reference-mode reversal's extra per-step work included); with
+    // reference-mode reversal's extra per-step work, measured at 0.9 of a
+    // forward step, included); with
     // sqrt_or_full_only (the batch engine, which runs no binomial schedule)
     // BINOMIAL only when SQRT does not fit.
     fkadj_status plan_trajectory(TrajPlan& tp, bool sqrt_or_full_only = false);

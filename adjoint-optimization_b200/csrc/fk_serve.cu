@@ -9,9 +9,24 @@
 // run share every launch with them.  Finished jobs hand their results back and
 // free their memory.  Waits on the client side are bounded.  The reference has
 // no serving path (one synchronous MATLAB call per gradient).
+//
+// Two ways to run the admitted requests (FKADJ_SERVE_MODE):
+//   streams (default)  a pool of worker threads (FKADJ_SERVE_STREAMS, 4), each
+//       taking the next admitted request and running it through the
+//       single-instance path on its own stream: the requests' kernels overlap
+//       on the device wherever SMs are free, and each request gets the
+//       single-instance kernels (one-wave tiles, kept f, bulk tile copies).
+//   ticks  one worker thread ticking a BatchEngine: every running request's
+//       next step joins one persistent launch per kernel kind.
+// Admission is the same: arrival order, while the estimated device footprint
+// fits the budget.  Measured on B200 the tick engine served a stream of
+// 128^2..512^2 requests slower than plain one-at-a-time solves, the stream
+// workers faster.
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <cstdlib>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -54,7 +69,12 @@ public:
 
 private:
     void loop();
+    void worker();
     fkadj_status admit(Request& r);
+    fkadj_status run_alone(Request& r);
+    bool streams_ = true;
+    int nworkers_ = 4;
+    std::vector<std::thread> workers_;
     fkadj_options opt_{};
     int device_ = 0;
     int64_t budget_ = 0, used_ = 0;
@@ -90,6 +110,12 @@ fkadj_status Server::start(const fkadj_options* opt, int64_t budget) {
         budget = (int64_t)(0.8 * (double)fr);
     }
     budget_ = budget;
+    if (const char* m = getenv("FKADJ_SERVE_MODE")) streams_ = std::strcmp(m, "ticks") != 0;
+    if (const char* w = getenv("FKADJ_SERVE_STREAMS")) nworkers_ = std::max(1, std::min(64, std::atoi(w)));
+    if (streams_) {
+        for (int k = 0; k < nworkers_; ++k) workers_.emplace_back([this] { worker(); });
+        return FKADJ_OK;
+    }
     std::unique_lock<std::mutex> lk(mu_);
     th_ = std::thread([this] { loop(); });
     cv_.wait(lk, [this] { return started_; });
@@ -97,10 +123,82 @@ fkadj_status Server::start(const fkadj_options* opt, int64_t budget) {
 }
 
 void Server::stop() {
-    if (!th_.joinable()) return;
     stop_ = true;
     cv_.notify_all();
-    th_.join();
+    for (auto& w : workers_)
+        if (w.joinable()) w.join();
+    workers_.clear();
+    if (th_.joinable()) th_.join();
+}
+
+// One request through the single-instance path on the worker's own problem
+// and stream: device memory from the per-device stream-ordered pool (no
+// device-wide synchronisation when it is freed), tiles from the autotuner's
+// cache for the grid shape.
+fkadj_status Server::run_alone(Request& r) {
+    auto pb = std::make_unique<Problem>();
+    pb->set_oneshot(oneshot_pool(&opt_));
+    fkadj_options o = opt_;
+    o.stream = nullptr;
+    o.device = device_;
+    o.ckpt_policy = opt_.ckpt_policy == FKADJ_CKPT_FULL ? FKADJ_CKPT_FULL : FKADJ_CKPT_SQRT;
+    o.ckpt_budget_bytes = budget_;
+    fkadj_status s = pb->init(r.p, r.dt, r.nt, r.ai.data(), r.nrows, r.ncols, r.n_num, r.gh.data(), r.gamma.data(),
+                              r.n_num, r.Jc.data(), r.Ir.data(), r.Sv.data(), r.alpha, &o, true);
+    if (s) return s;
+    if (r.want_grad) {
+        std::vector<double> g(r.nt + 1);
+        s = pb->grad(r.Et.data(), r.y0.data(), &r.L0, &r.LE, &r.Lcost, g.data(), nullptr);
+        r.gradE.swap(g);
+    } else {
+        s = pb->objective(r.Et.data(), r.y0.data(), &r.L0, &r.LE, &r.Lcost, nullptr);
+    }
+    return s;
+}
+
+void Server::worker() {
+    if (cudaSetDevice(device_) != cudaSuccess) return;
+    while (true) {
+        int64_t id = 0;
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            // the front request, once its footprint fits beside the running ones
+            cv_.wait(lk, [this] {
+                if (stop_) return true;
+                if (queue_.empty()) return false;
+                const Request& f = *reqs_[queue_.front()];
+                return running_.empty() || used_ + f.est <= budget_;
+            });
+            if (stop_ && queue_.empty()) return;
+            if (queue_.empty()) continue;
+            id = queue_.front();
+            queue_.pop_front();
+            r = reqs_[id].get();
+            r->state = 1;
+            r->t_admit = host_seconds();
+            used_ += r->est;
+            running_.push_back(id);
+            peak_running_ = std::max<int64_t>(peak_running_, (int64_t)running_.size());
+        }
+        const fkadj_status s = run_alone(*r);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            r->status = s;
+            r->state = (s == FKADJ_OK || s == FKADJ_ERR_NUMERIC) ? 2 : 3;
+            if (r->state == 3) {
+                r->err = fkadj_last_error();
+                ++failed_;
+            } else {
+                ++completed_;
+            }
+            r->t_done = host_seconds();
+            used_ -= r->est;
+            running_.erase(std::find(running_.begin(), running_.end(), id));
+        }
+        done_cv_.notify_all();
+        cv_.notify_all();  // memory freed: the next request may fit now
+    }
 }
 
 fkadj_status Server::submit(std::unique_ptr<Request> r, int64_t* id) {

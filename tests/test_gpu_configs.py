@@ -5,9 +5,11 @@ round-off growth allows (tests/chaos_horizon.py measures them).
       2000 RK4 steps, 20 holes r~U(0.02, 0.08) cm, one broken wavefront,
       E over 100 intervals, J = mean u(T)^2: the whole horizon.
   C2  fkadj.workloads.large_instance(): 512^2, 200 holes r~U(0.02, 0.1) cm,
-      8 broken wavefronts, E over 400 intervals (of 20000 steps): its first
-      C2_HORIZON steps, the longest at which the reference comparison holds
-      its tolerances on the measured growth.
+      8 broken wavefronts, E over 400 intervals, 20000 steps: the forward
+      states over the whole horizon against the reference binary; the gradient
+      against the reference binary over its first 2500 steps (the longest its
+      int trajectory offset allows) and against the oracle over the first
+      C2_HORIZON steps (the oracle's run time).
 
 Each is checked against the reference's own CUDA code compiled here
 (oracle/_ref, skipped where absent) and against the CPU oracle: states
@@ -25,8 +27,13 @@ from fkadj import _lib, api, workloads as W
 
 pytestmark = pytest.mark.gpu
 
-# steps of the C2 instance the reference and the oracle comparisons run for
+# steps of the C2 instance the oracle comparisons run for (the oracle's 512^2
+# gradient costs about 14 ms per step on 16 cores)
 C2_HORIZON = 2000
+# the reference binary's gradient addresses its host trajectory with a 32-bit
+# int offset, (i+1)*3*n (src/cuda/fk_grad_Et_mono_PARAMETERS.cu:1720, 1871),
+# which overflows past 2729 steps at 512^2: its comparison runs to 2500 steps
+C2_REF_GRAD_HORIZON = 2500
 
 
 def _truncate(inst, T):
@@ -108,6 +115,34 @@ def test_c2_forward_states_at_the_parity_horizon(c2):
 
 def test_c2_gradient_at_the_parity_horizon(c2):
     _check_gradient(c2)
+
+
+@pytest.mark.skipif(not refbin.available(), reason="oracle/_ref not built")
+def test_c2_forward_states_over_the_whole_horizon_against_the_reference_binary():
+    """All 20000 steps of C2 against the reference's own CUDA forward: the
+    measured round-off growth (tests/chaos_horizon.py: about 0.07 decades per
+    1000 steps) keeps the states within 1e-10 at every snapshot."""
+    inst = W.large_instance()
+    nstep = 5000
+    ns = api.compute_ns(inst.nt, nstep)
+    ys, yf, _ = api.fk_forward_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                                  inst.ghost, nstep, params=inst.params)
+    ys_r, yf_r = refbin.forward(inst.dt, inst.Et, inst.nt, inst.y0, inst.active_index, inst.nrows, inst.ncols,
+                                inst.ghost, nstep, ns)
+    assert _rel(yf, yf_r) <= 1e-10
+    for k in range(ns):
+        assert _rel(ys[:, k], ys_r[k]) <= 1e-10
+
+
+@pytest.mark.skipif(not refbin.available(), reason="oracle/_ref not built")
+def test_c2_gradient_against_the_reference_binary_at_its_longest_horizon():
+    inst = _truncate(W.large_instance(), C2_REF_GRAD_HORIZON)
+    g, Lc, _, _, _ = api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                                    inst.ghost, inst.gamma, inst.S, inst.alpha, params=inst.params)
+    r = refbin.grad(inst.dt, inst.Et, inst.nt, inst.y0, inst.active_index, inst.nrows, inst.ncols, inst.ghost,
+                    inst.gamma, inst.S, inst.alpha)
+    assert abs(Lc - r["Lcost"]) <= 1e-10 * abs(r["Lcost"])
+    assert _rel2(g, r["gradE"]) <= 1e-8
 
 
 def test_c2_exact_gradient_central_fd_on_10_seeded_intervals(c2):

@@ -218,18 +218,19 @@ def test_windowed_zgh_reduction_matches_oracle_and_batch(mode):
 @pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
 def test_auto_store_takes_the_schedule_that_recomputes_less(mode):
     """AUTO with a budget below the full trajectory (131 states): 100 states
-    let the binomial schedule recompute 32 steps against sqrt's 119, so it is
-    taken in both modes; with 30 states binomial recomputes 102, which the
-    exact mode still prefers, while the reference mode (whose binomial
-    reversal also loses the kept k1 and copies a state per step) keeps sqrt.
-    Every choice gives the bits of full storage."""
-    inst = _inst(48, 130, seed=23, ncols=64, objective="gradient")
+    let the binomial schedule recompute 32 steps against sqrt's 119, 30 states
+    102.  The exact mode takes binomial both times; the reference mode, whose
+    binomial reversal also loses the kept k1 and copies a state per step (0.9
+    of a forward step per backward step, as measured), keeps sqrt.  Every
+    choice gives the bits of full storage."""
+    inst = _inst(48, 130, seed=23, ncols=64, objective="gradient", alpha=0.2)
     args = (inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows, inst.ghost,
-            inst.gamma, inst.S, 0.2)
+            inst.gamma, inst.S, inst.alpha)
     full = api.fk_grad_Et(*args, params=inst.params,
                           opts=api.options(grad_mode=mode, ckpt_policy=_lib.CKPT_FULL))
     sb = _state_bytes(inst.nrows, inst.ncols)
-    for states, want in ((100, "binomial"), (30, "binomial" if mode == _lib.GRAD_EXACT else "sqrt")):
+    want = "binomial" if mode == _lib.GRAD_EXACT else "sqrt"
+    for states in (100, 30):
         opts = api.options(grad_mode=mode, ckpt_policy=_lib.CKPT_AUTO, ckpt_budget_bytes=states * sb)
         with api.Problem(inst, opts=opts) as pb:
             r = pb.grad(inst.Et, inst.y0)
