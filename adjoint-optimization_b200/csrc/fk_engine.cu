@@ -354,6 +354,28 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
         if (t >= 0 && t < fused_count()) tkf_ = t;
     }
     adj_path_ = forced_path_ >= 0 ? forced_path_ : ADJ_SPLIT;
+    // FKADJ_TILES=f[:rows],m[:rows],a,e fixes the preset (index into the tile
+    // list) of each kernel kind, and the forward step's and midpoint's rows per
+    // tile, instead of autotuning: a profiler run then measures the kernels the
+    // autotuner picks without the profiler (whose timings mislead it).
+    if (const char* tl = getenv("FKADJ_TILES")) {
+        int k = 0;
+        for (const char* q = tl; *q && k < 4; ++k) {
+            char* end = nullptr;
+            const long t = std::strtol(q, &end, 10);
+            if (end == q || t < 0 || t >= tile_count()) break;
+            tk_[k] = (int)t;
+            ty_[k] = 0;
+            q = end;
+            if (*q == ':') {
+                const long r = std::strtol(q + 1, &end, 10);
+                if (r > 0 && r <= tile_shape((int)t).ty && (k == T_FWD || k == T_MID)) ty_[k] = (int)r;
+                q = end;
+            }
+            if (*q == ',') ++q;
+        }
+        if (k == 4) autotune_ = false, tuned_ = true;
+    }
     subblock_lattice(g_, &nsbx_, &nsby_);
     nsb_ = nsbx_ * nsby_;
 

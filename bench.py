@@ -391,6 +391,7 @@ def run_ours(args):
                                 grad_mode=gmode)
             with api.Problem(inst, opts=fopts) as pf:
                 pf.grad(Et, inst.y0)
+                pf.grad(Et)  # the second call captures the gradient's graph: outside the timed region
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 torch.cuda.synchronize()
                 e0.record(stream)
@@ -412,6 +413,7 @@ def run_ours(args):
                                 grad_mode=gmode)
             with api.Problem(inst, opts=aopts) as pa:
                 pa.grad(Et, inst.y0)
+                pa.grad(Et)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 torch.cuda.synchronize()
                 e0.record(stream)
@@ -478,6 +480,7 @@ def serve_and_batch(args):
     """Served stream and batched uneven instances (scaled down from the
     standard 128-1024 sides and 1000-20000 steps so the bench stays within
     minutes; the keys say how)."""
+    import numpy as np
     from fkadj import suite
     from fkadj import workloads as W
     base, grads, rng = suite.serve_requests(args.serve_requests, 7, args.serve_max_side, args.serve_nt_scale)
@@ -497,10 +500,24 @@ def serve_and_batch(args):
                         for r in rows])
     insts = W.batch_instances(count=args.batch_count, seed=2, max_side=args.serve_max_side,
                               nt_scale=args.serve_nt_scale)
-    batched = suite.batch_measure(insts)
-    batched["scale"] = (f"{args.batch_count} of the 64 uneven instances, sides <= {args.serve_max_side}, "
-                        f"horizons x{args.serve_nt_scale}")
-    batched["sequential"] = "one resident problem at a time, each gradient a replayed graph"
+    ticks = suite.batch_measure(insts)
+    # the same gradients as one burst of requests to the server: its workers run
+    # them concurrently through the single-instance path, one stream each
+    stream_rows = suite.serve_measure(insts, [True] * len(insts), [float("inf")], np.random.default_rng(3))
+    r = stream_rows[0]
+    streams = {"gradients_per_s": len(insts) / (len(insts) / r["served_throughput_req_s"]),
+               "makespan_s": len(insts) / r["served_throughput_req_s"],
+               "speedup": r["served_throughput_req_s"] / r["sequential_warm_throughput_req_s"],
+               "sequential_warm_gradients_per_s": r["sequential_warm_throughput_req_s"],
+               "what": "every gradient submitted at once to the server (concurrent single-instance solves, one "
+                       "stream each, admission by device footprint)"}
+    ticks["what"] = "one BatchEngine: every tick's steps of all jobs in one persistent launch per kernel kind"
+    best = max((streams, ticks), key=lambda x: x["speedup"])
+    batched = {"count": len(insts), "sides": ticks["sides"], "nt_range": ticks["nt_range"],
+               "scale": (f"{args.batch_count} of the 64 uneven instances, sides <= {args.serve_max_side}, "
+                         f"horizons x{args.serve_nt_scale}"),
+               "sequential": "one resident problem at a time, each gradient a replayed graph",
+               "speedup": best["speedup"], "streams": streams, "persistent_kernels": ticks}
     return served, plain, batched
 
 

@@ -1,6 +1,7 @@
 """Serving (fkadj_server_*): requests of different sizes arriving while others
-run are admitted and computed together; each result equals the one-shot
-result and is the same alone and in the mix; waits are bounded."""
+run are admitted and computed together (concurrent single-instance solves on
+a pool of streams, or the tick engine's batched launches); each result equals
+the one-shot result and is the same alone and in the mix; waits are bounded."""
 import threading
 import time
 
@@ -21,7 +22,12 @@ def _requests(seed):
             for k, (nr, nc, nt, g) in enumerate(specs)]
 
 
-def test_served_results_match_one_shot_and_are_mix_invariant():
+@pytest.mark.parametrize("mode", ["streams", "ticks"])
+def test_served_results_match_one_shot_and_are_mix_invariant(monkeypatch, mode):
+    """Both ways of running admitted requests: concurrent single-instance
+    solves on a pool of streams (the default) and the tick engine's batched
+    launches (FKADJ_SERVE_MODE=ticks)."""
+    monkeypatch.setenv("FKADJ_SERVE_MODE", mode)
     reqs = _requests(300)
     target, _ = reqs[0]
     with Server() as srv:
@@ -61,7 +67,9 @@ def test_served_results_match_one_shot_and_are_mix_invariant():
         assert res["latency_s"] >= res["queue_s"] >= 0
 
 
-def test_admission_respects_the_hbm_budget():
+@pytest.mark.parametrize("mode", ["streams", "ticks"])
+def test_admission_respects_the_hbm_budget(monkeypatch, mode):
+    monkeypatch.setenv("FKADJ_SERVE_MODE", mode)
     reqs = _requests(400)
     # a budget that fits about two of these requests at a time
     with Server(hbm_budget_bytes=25_000_000) as srv:
