@@ -66,7 +66,7 @@ FUSED_BYTES_PER_CELL = {"fused": 266.0, "fused-recompute": 154.0}
 EXACT_BYTES_PER_CELL = 153.0
 # FP64 flops per vector-field evaluation of the forward step (stage update included), counted by ncu
 # (2 x DFMA + DMUL + DADD thread instructions) at 512x512
-FWD_FLOPS_PER_EVAL = 740.4 / 4.58984375
+FWD_FLOPS_PER_EVAL = 693.6 / 4.58984375
 
 
 def fwd_evaluations(nrows, ncols, tx, ty):
