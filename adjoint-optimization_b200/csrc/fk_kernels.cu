@@ -56,6 +56,12 @@ constexpr int kLoadUnroll = FKADJ_LOAD_UNROLL;
 #ifndef FKADJ_BATCH_ONE_CTA
 #define FKADJ_BATCH_ONE_CTA 0
 #endif
+// The single-instance adjoint step's stage loops load the next cell's global
+// operands while the current one computes (see adj_stage; the batched kernels,
+// short of registers, keep the plain loop).
+#ifndef FKADJ_ADJ_PREFETCH
+#define FKADJ_ADJ_PREFETCH 0
+#endif
 #define FKADJ_BATCH_MINB(tx, ty, nt) (FKADJ_BATCH_ONE_CTA ? 1 : min_blocks(tx, ty, nt))
 
 constexpr int kStageUnroll = FKADJ_STAGE_UNROLL;
@@ -485,7 +491,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
 // The Jacobian comes from the cache jload when it is non-null, else it is
 // evaluated at ys; jstore (non-null only in the last stage) keeps the evaluated
 // one for the next backward step.
-template <int E, int TX, int TY, int NT, int MODE>
+template <int E, int TX, int TY, int NT, int MODE, bool PF = false>
 __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, const double* __restrict__ src,
                                           double* __restrict__ dst, double* __restrict__ D,
                                           const double* __restrict__ z0g, const uint8_t* __restrict__ wc,
@@ -495,35 +501,9 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
     constexpr int IN = TX * TY;
-    RowCol<W, NT> rc(HALO - E, HALO - E);
-#pragma unroll kStageUnroll
-    for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
-        const int r = rc.r, c = rc.c;
-        const int s = r * RW + c;
-        const long long o = off + (long long)r * g.ld + c;
-        double a, b, e;
-        if (MODE == 0) {  // the first stage's source region is z0 itself
-            a = src[s], b = src[RN + s], e = src[2 * RN + s];
-        } else {
-            a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
-        }
-        const int code = __ldg(wc + o);
-        double ku, kv, kw;
-#if FKADJ_HOLE_BRANCH
-        if (isnan(src[s])) {  // holes and the NaN ring: the result is NaN
-            ku = kv = kw = src[s];
-        } else
-#endif
-        {
-            JacT J;
-            if (jload) {
-                J = load_jac(jload, g.plane, o);
-            } else {
-                J = fk_jacT(P, finite_u(__ldg(ys + o)), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
-                if (jstore) store_jac(jstore, g.plane, o, J);
-            }
-            adj_at<RW, RN>(P, src, s, code, J, ku, kv, kw);
-        }
+    // the stage update of cell (r, c) from its step-start value and k
+    auto finish = [&](int r, int c, int s, long long o, double a, double b, double e, double ku, double kv,
+                      double kw) {
         const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
@@ -549,6 +529,85 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
                 }
             }
         }
+    };
+    RowCol<W, NT> rc(HALO - E, HALO - E);
+    if constexpr (PF) {
+        // Software-pipelined (the single-instance kernel): the next cell's
+        // global operands (step-start state, weight code, cached Jacobian or
+        // the state it is evaluated at) are loaded while this cell computes.
+        struct Ops {
+            double a, b, e, j[7];
+            int code;
+        };
+        auto fetch = [&](int r, int c, Ops& x) {
+            const long long o = off + (long long)r * g.ld + c;
+            if (MODE != 0) x.a = __ldg(z0g + o), x.b = __ldg(z0g + g.plane + o), x.e = __ldg(z0g + 2 * g.plane + o);
+            x.code = __ldg(wc + o);
+            if (jload) {
+#pragma unroll
+                for (int k = 0; k < 7; ++k) x.j[k] = __ldg(jload + k * g.plane + o);
+            } else {
+                x.j[0] = __ldg(ys + o), x.j[1] = __ldg(ys + g.plane + o), x.j[2] = __ldg(ys + 2 * g.plane + o);
+            }
+        };
+        Ops cur;
+        if ((int)threadIdx.x < N) fetch(rc.r, rc.c, cur);
+        for (int q = threadIdx.x; q < N; q += NT) {
+            const int r = rc.r, c = rc.c;
+            rc.next();
+            Ops nxt;
+            if (q + NT < N) fetch(rc.r, rc.c, nxt);
+            const int s = r * RW + c;
+            const long long o = off + (long long)r * g.ld + c;
+            double a = cur.a, b = cur.b, e = cur.e;
+            if (MODE == 0) a = src[s], b = src[RN + s], e = src[2 * RN + s];
+            double ku, kv, kw;
+            if (isnan(src[s])) {  // holes and the NaN ring: the result is NaN
+                ku = kv = kw = src[s];
+            } else {
+                JacT J;
+                if (jload) {
+                    J = {cur.j[0], cur.j[1], cur.j[2], cur.j[3], cur.j[4], cur.j[5], cur.j[6]};
+                } else {
+                    J = fk_jacT(P, finite_u(cur.j[0]), cur.j[1], cur.j[2]);
+                    if (jstore) store_jac(jstore, g.plane, o, J);
+                }
+                adj_at<RW, RN>(P, src, s, cur.code, J, ku, kv, kw);
+            }
+            finish(r, c, s, o, a, b, e, ku, kv, kw);
+            cur = nxt;
+        }
+    } else {
+#pragma unroll kStageUnroll
+        for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
+            const int r = rc.r, c = rc.c;
+            const int s = r * RW + c;
+            const long long o = off + (long long)r * g.ld + c;
+            double a, b, e;
+            if (MODE == 0) {  // the first stage's source region is z0 itself
+                a = src[s], b = src[RN + s], e = src[2 * RN + s];
+            } else {
+                a = __ldg(z0g + o), b = __ldg(z0g + g.plane + o), e = __ldg(z0g + 2 * g.plane + o);
+            }
+            const int code = __ldg(wc + o);
+            double ku, kv, kw;
+#if FKADJ_HOLE_BRANCH
+            if (isnan(src[s])) {  // holes and the NaN ring: the result is NaN
+                ku = kv = kw = src[s];
+            } else
+#endif
+            {
+                JacT J;
+                if (jload) {
+                    J = load_jac(jload, g.plane, o);
+                } else {
+                    J = fk_jacT(P, finite_u(__ldg(ys + o)), __ldg(ys + g.plane + o), __ldg(ys + 2 * g.plane + o));
+                    if (jstore) store_jac(jstore, g.plane, o, J);
+                }
+                adj_at<RW, RN>(P, src, s, code, J, ku, kv, kw);
+            }
+            finish(r, c, s, o, a, b, e, ku, kv, kw);
+        }
     }
     if (MODE != 2) __syncthreads();
 }
@@ -559,7 +618,7 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
 // Jacobian caches (null = evaluate): jb = J(y_i) left by the previous step's
 // last stage, jh = J(yh) from k_adj_mid; J(y_{i-1}) is evaluated in the last
 // stage and stored to ja for the next step.
-template <int TX, int TY, int NT, bool BULK = false>
+template <int TX, int TY, int NT, bool BULK = false, bool PF = false>
 __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ z,
                                               double* __restrict__ zout, const double* __restrict__ yb,
                                               const double* __restrict__ yh, const double* __restrict__ ya,
@@ -579,10 +638,12 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
                                         nullptr, phase))
         return;
     const double dt = P.dt;
-    adj_stage<3, TX, TY, NT, 0>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb, nullptr);
-    adj_stage<2, TX, TY, NT, 1>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
-    adj_stage<1, TX, TY, NT, 1>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
-    adj_stage<0, TX, TY, NT, 2>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, nullptr, ja);
+    adj_stage<3, TX, TY, NT, 0, PF>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb,
+                                    nullptr);
+    adj_stage<2, TX, TY, NT, 1, PF>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh,
+                                    nullptr);
+    adj_stage<1, TX, TY, NT, 1, PF>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
+    adj_stage<0, TX, TY, NT, 2, PF>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, nullptr, ja);
     __syncthreads();
     subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
 }
@@ -595,8 +656,8 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja,
                unsigned* fault) {
     pdl_enter();
-    adj_step_tile<TX, TY, NT, true>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, blockIdx.x, blockIdx.y,
-                                    fault);
+    adj_step_tile<TX, TY, NT, true, FKADJ_ADJ_PREFETCH != 0>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh,
+                                                             ja, blockIdx.x, blockIdx.y, fault);
 }
 
 // ------------------------------------------- fused reference-mode adjoint
