@@ -28,6 +28,15 @@
 #ifndef FKADJ_MERGED_TVM
 #define FKADJ_MERGED_TVM 1
 #endif
+// Smoothed steps without their overflow tests (see step_of_exp)
+#ifndef FKADJ_FAST_STEPS
+#define FKADJ_FAST_STEPS 0
+#endif
+// Mirrored neighbours of v and w read at offsets chosen from u's NaN tests
+// (1), u's too (2), instead of selected among all four (0; see rhs_at)
+#ifndef FKADJ_MIRROR_OFFSETS
+#define FKADJ_MIRROR_OFFSETS 0
+#endif
 
 namespace fkadj {
 
@@ -41,6 +50,7 @@ struct DevModel {
     double r_tau_d, r_tau_0, r_tau_r, r_2tau_si;
     double tau_v1m, tau_v2m, r_tau_vp, r_tau_wm, r_tau_wp;
     double r_tau_v2m;  // 1 / tau_v2_minus
+    double m2ksm, m2kfk;  // -2 ksm, -2 k_fk: -2 (k x) = (-2 k) x exactly
     double dv12;  // tau_v2_minus - tau_v1_minus
     double eq;    // exp(-2 ksm (u_c - u_v)): e^{-2ksm(u-u_v)} = eq * e^{-2ksm(u-u_c)}
     double cu, cv, cw;  // D / h^2
@@ -96,6 +106,20 @@ __device__ __forceinline__ double fk_rcp(double x) {
 #endif
 }
 
+// own_rcp for finite x in [1, 2^1001]: the same value, without the +inf test.
+__device__ __forceinline__ double fk_rcp_finite(double x) {
+#if FKADJ_OWN_RCP
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+#else
+    return 1.0 / x;
+#endif
+}
+
 // Smoothed step s = (1 + tanh x)/2 written as the logistic 1/(1 + e^{-2x})
 // (the same function; one exp and one reciprocal instead of a tanh) and its
 // complement 1 - s = e^{-2x} s without cancellation.  e^{-2x} overflows to
@@ -103,12 +127,33 @@ __device__ __forceinline__ double fk_rcp(double x) {
 struct Step {
     double s, c;  // s and 1 - s
 };
+//
+// FKADJ_FAST_STEPS: e is capped at 2^1000 first, so 1 + e stays finite and s
+// positive, and neither the reciprocal's +inf test nor the s = 0 test is
+// needed.  Below the cap (|x| < 346, i.e. u more than 3.4 below u_c for the
+// p step: far outside the model's range) the value is the same to the bit;
+// above it s is 2^-1000 instead of 0 and 1 - s is 1.
 __device__ __forceinline__ Step step_of_exp(double e) {
+#if FKADJ_FAST_STEPS
+    e = fmin(e, 0x1p1000);
+    const double s = fk_rcp_finite(1.0 + e);
+    return {s, e * s};
+#else
     const double s = fk_rcp(1.0 + e);
     // s = 0 when 1 + e is +inf, or (own reciprocal) beyond 2^1022
     return {s, s == 0.0 ? 1.0 : e * s};
+#endif
 }
 __device__ __forceinline__ Step smooth_step(double x) { return step_of_exp(exp(-2.0 * x)); }
+
+// e^{-2 k (u - u0)} as the smoothed steps take it; m2k = -2 k (the same product)
+__device__ __forceinline__ double step_exp(double m2k, double k, double u, double u0) {
+#if FKADJ_FAST_STEPS
+    return exp(m2k * (u - u0));
+#else
+    return exp(-2.0 * (k * (u - u0)));
+#endif
+}
 
 // p and q share the slope ksm, so q's exponential is p's times a constant:
 // one exp for both.
@@ -138,7 +183,11 @@ struct TvmRcp {
 };
 __device__ __forceinline__ TvmRcp tvm_rcp(const DevModel& P, double eq) {
     if (eq > 1e300) return {P.r_tau_v2m, 0.0};
+#if FKADJ_FAST_STEPS
+    const double rT = fk_rcp_finite(fma(eq, P.tau_v2m, P.tau_v1m));  // finite: eq <= 1e300
+#else
     const double rT = fk_rcp(fma(eq, P.tau_v2m, P.tau_v1m));
+#endif
     return {(1.0 + eq) * rT, (4.0 * eq) * (rT * rT)};
 }
 
@@ -147,7 +196,7 @@ __device__ __forceinline__ TvmRcp tvm_rcp(const DevModel& P, double eq) {
 __device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, double w,
                                        double& ud, double& vd, double& wd) {
 #if FKADJ_MERGED_TVM
-    const double e = exp(-2.0 * (P.ksm * (u - P.u_c)));
+    const double e = step_exp(P.m2ksm, P.ksm, u, P.u_c);
     const Step sp = step_of_exp(e);
     const double rtvm = tvm_rcp(P, e * P.eq).r;
 #else
@@ -157,7 +206,7 @@ __device__ __forceinline__ void fk_ion(const DevModel& P, double u, double v, do
     const double tvm = q * P.tau_v1m + sq.c * P.tau_v2m;
     const double rtvm = fk_rcp(tvm);
 #endif
-    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
+    const Step ss = step_of_exp(step_exp(P.m2kfk, P.k_fk, u, P.u_csi));
     const double p = sp.s;
     const double j_fi = -v * p * (1.0 - u) * (u - P.u_c) * P.r_tau_d;
     const double j_so = u * sp.c * P.r_tau_0 + p * P.r_tau_r;
@@ -177,7 +226,7 @@ struct JacT {
 // 1 - tanh^2 = 4 s (1 - s) for the smoothed step s.
 __device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, double w) {
 #if FKADJ_MERGED_TVM
-    const double e = exp(-2.0 * (P.ksm * (u - P.u_c)));
+    const double e = step_exp(P.m2ksm, P.ksm, u, P.u_c);
     const Step sp = step_of_exp(e);
     const TvmRcp tv = tvm_rcp(P, e * P.eq);
     const double rtvm = tv.r, dq_rtvm2 = tv.dqr;
@@ -190,7 +239,7 @@ __device__ __forceinline__ JacT fk_jacT(const DevModel& P, double u, double v, d
     const double rtvm = fk_rcp(tvm);
     const double dq_rtvm2 = dq * (rtvm * rtvm);
 #endif
-    const Step ss = smooth_step(P.k_fk * (u - P.u_csi));
+    const Step ss = step_of_exp(step_exp(P.m2kfk, P.k_fk, u, P.u_csi));
     const double p = sp.s;
     const double dp = 4.0 * sp.s * sp.c;
     const double ds = 4.0 * ss.s * ss.c;
@@ -265,6 +314,21 @@ __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restri
     const double un = Y[q - W], us = Y[q + W], uw = Y[q - 1], ue = Y[q + 1];
     const bool nN = isnan(un), nS = !nN && isnan(us);
     const bool nW = isnan(uw), nE = !nW && isnan(ue);
+#if FKADJ_MIRROR_OFFSETS
+    // the same neighbours as the selects below, read where they are
+    const int qa = nN ? q + W : q - W, qb = nS ? q - W : q + W;
+    const int qc = nW ? q + 1 : q - 1, qd = nE ? q - 1 : q + 1;
+#if FKADJ_MIRROR_OFFSETS == 2
+    const double a_u = Y[qa], b_u = Y[qb], c_u = Y[qc], d_u = Y[qd];
+#else
+    const double a_u = nN ? us : un, b_u = nS ? un : us, c_u = nW ? ue : uw, d_u = nE ? uw : ue;
+#endif
+    const double* Yv = Y + RN;
+    const double* Yw = Y + 2 * RN;
+    const double lu = P.cu * ((((a_u + b_u) + c_u) + d_u) - 4.0 * u);
+    const double lv = P.cv * ((((Yv[qa] + Yv[qb]) + Yv[qc]) + Yv[qd]) - 4.0 * v);
+    const double lw = P.cw * ((((Yw[qa] + Yw[qb]) + Yw[qc]) + Yw[qd]) - 4.0 * w);
+#else
     const double vn = Y[RN + q - W], vs = Y[RN + q + W], vw = Y[RN + q - 1], ve = Y[RN + q + 1];
     const double wn = Y[2 * RN + q - W], ws = Y[2 * RN + q + W], ww = Y[2 * RN + q - 1],
                  we = Y[2 * RN + q + 1];
@@ -276,6 +340,7 @@ __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restri
     const double lu = P.cu * ((((a_u + b_u) + c_u) + d_u) - 4.0 * u);
     const double lv = P.cv * ((((a_v + b_v) + c_v) + d_v) - 4.0 * v);
     const double lw = P.cw * ((((a_w + b_w) + c_w) + d_w) - 4.0 * w);
+#endif
     double ud, vd, wd;
     fk_ion(P, finite_u(u), v, w, ud, vd, wd);
     fu = (lu + ud) + Egh;

@@ -44,6 +44,8 @@ static DevModel make_model(const fkadj_params& p, double dt) {
     M.tau_v1m = p.tau_v1_minus;
     M.tau_v2m = p.tau_v2_minus;
     M.r_tau_v2m = 1.0 / p.tau_v2_minus;
+    M.m2ksm = -2.0 * p.ksm;
+    M.m2kfk = -2.0 * p.k_fk;
     M.r_tau_vp = 1.0 / p.tau_v_plus;
     M.r_tau_wm = 1.0 / p.tau_w_minus;
     M.r_tau_wp = 1.0 / p.tau_w_plus;

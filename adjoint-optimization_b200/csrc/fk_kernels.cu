@@ -56,9 +56,9 @@ constexpr int kLoadUnroll = FKADJ_LOAD_UNROLL;
 #ifndef FKADJ_BATCH_ONE_CTA
 #define FKADJ_BATCH_ONE_CTA 0
 #endif
-// The single-instance adjoint step's stage loops load the next cell's global
-// operands while the current one computes (see adj_stage; the batched kernels,
-// short of registers, keep the plain loop).
+// The single-instance midpoint and adjoint-step kernels load the next cell's
+// global operands while the current one computes (adj_mid_tile's first loop,
+// adj_stage; the batched kernels, short of registers, keep the plain loops).
 #ifndef FKADJ_ADJ_PREFETCH
 #define FKADJ_ADJ_PREFETCH 0
 #endif
@@ -380,7 +380,7 @@ __device__ __forceinline__ void store_jac(double* __restrict__ Jb, long long pla
 //   f(ya, Ea) is k1 of the forward step from ya: when fa is non-null (the
 //   forward recompute kept it) it is read from there too;
 //   J_F(yh)^T, used by stages 2 and 3 of the adjoint step, goes to jh.
-template <int TX, int TY, int NT, bool BULK = false>
+template <int TX, int TY, int NT, bool BULK = false, bool PF = false>
 __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ ya,
                                              const double* __restrict__ yb, const double* __restrict__ gh,
                                              double* __restrict__ yh, double Ea, double Eb, double E3,
@@ -407,28 +407,8 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
     {
         constexpr int W = TX + 2;
         const int N = W * (rows + 2);
-        RowCol<W, NT> rc(1, 1);
-#pragma unroll kStageUnroll
-        for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
-            const int r = rc.r, c = rc.c;
-            const int s = r * RW + c;
-            const long long o = off + (long long)r * g.ld + c;
-            const double gg = __ldg(gh + o);
-            double a0[3], a1[3];
-            if (fa) {
-                a0[0] = __ldg(fa + o);
-                a0[1] = __ldg(fa + g.plane + o);
-                a0[2] = __ldg(fa + 2 * g.plane + o);
-            } else {
-                rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
-            }
-            if (fin) {
-                a1[0] = __ldg(fin + o);
-                a1[1] = __ldg(fin + g.plane + o);
-                a1[2] = __ldg(fin + 2 * g.plane + o);
-            } else {
-                rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
-            }
+        // Hermite parts of cell (r, c) from f(ya) = a0 and f(yb) = a1
+        auto hermite = [&](int r, int c, int s, long long o, const double* a0, const double* a1) {
             const bool inner = r >= H2 && r < H2 + rows && c >= H2 && c < H2 + TX;
             if (inner && fout) {
                 fout[o] = a0[0];
@@ -444,6 +424,60 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
                     Q[f * TX * TY + (r - H2) * TX + (c - H2)] =
                         ((hw.c4[0] * x0 + hw.c4[1] * m0) + hw.c4[2] * x1) + hw.c4[3] * m1;
                 }
+            }
+        };
+        RowCol<W, NT> rc(1, 1);
+        if constexpr (PF) {
+            // Software-pipelined (the single-instance kernel): gh and the kept
+            // f values of the next cell are loaded while this cell computes.
+            struct Ops {
+                double gg, a0[3], a1[3];
+            };
+            auto fetch = [&](int r, int c, Ops& x) {
+                const long long o = off + (long long)r * g.ld + c;
+                x.gg = __ldg(gh + o);
+                if (fa) x.a0[0] = __ldg(fa + o), x.a0[1] = __ldg(fa + g.plane + o), x.a0[2] = __ldg(fa + 2 * g.plane + o);
+                if (fin)
+                    x.a1[0] = __ldg(fin + o), x.a1[1] = __ldg(fin + g.plane + o), x.a1[2] = __ldg(fin + 2 * g.plane + o);
+            };
+            Ops cur;
+            if ((int)threadIdx.x < N) fetch(rc.r, rc.c, cur);
+            for (int q = threadIdx.x; q < N; q += NT) {
+                const int r = rc.r, c = rc.c;
+                rc.next();
+                Ops nxt;
+                if (q + NT < N) fetch(rc.r, rc.c, nxt);
+                const int s = r * RW + c;
+                const long long o = off + (long long)r * g.ld + c;
+                const int code = g.fcode ? (int)__ldg(g.fcode + o) : -1;
+                if (!fa) rhs_at<RW, RN>(P, A, s, Ea * cur.gg, cur.a0[0], cur.a0[1], cur.a0[2], code);
+                if (!fin) rhs_at<RW, RN>(P, B, s, Eb * cur.gg, cur.a1[0], cur.a1[1], cur.a1[2], code);
+                hermite(r, c, s, o, cur.a0, cur.a1);
+                cur = nxt;
+            }
+        } else {
+#pragma unroll kStageUnroll
+            for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
+                const int r = rc.r, c = rc.c;
+                const int s = r * RW + c;
+                const long long o = off + (long long)r * g.ld + c;
+                const double gg = __ldg(gh + o);
+                double a0[3], a1[3];
+                if (fa) {
+                    a0[0] = __ldg(fa + o);
+                    a0[1] = __ldg(fa + g.plane + o);
+                    a0[2] = __ldg(fa + 2 * g.plane + o);
+                } else {
+                    rhs_at<RW, RN>(P, A, s, Ea * gg, a0[0], a0[1], a0[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
+                }
+                if (fin) {
+                    a1[0] = __ldg(fin + o);
+                    a1[1] = __ldg(fin + g.plane + o);
+                    a1[2] = __ldg(fin + 2 * g.plane + o);
+                } else {
+                    rhs_at<RW, RN>(P, B, s, Eb * gg, a1[0], a1[1], a1[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
+                }
+                hermite(r, c, s, o, a0, a1);
             }
         }
     }
@@ -477,8 +511,8 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
               const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty,
               const double* __restrict__ fa, unsigned* fault) {
     pdl_enter();
-    adj_mid_tile<TX, TY, NT, true>(P, g, ya, yb, gh, yh, E.a(), E.b(), E.c(), hw, fin, fout, jh, blockIdx.x, blockIdx.y,
-                                   ty, fa, fault);
+    adj_mid_tile<TX, TY, NT, true, FKADJ_ADJ_PREFETCH != 0>(P, g, ya, yb, gh, yh, E.a(), E.b(), E.c(), hw, fin, fout,
+                                                            jh, blockIdx.x, blockIdx.y, ty, fa, fault);
 }
 
 // One adjoint stage on the tile grown by E cells: k = L^T src + J_F(y)^T src,
