@@ -350,6 +350,11 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
         else if (!std::strcmp(ap, "fused")) forced_path_ = ADJ_FUSED;
         else if (!std::strcmp(ap, "fused-recompute")) forced_path_ = ADJ_FUSED_RECOMPUTE;
     }
+    jcache_mode_ = 2;
+    if (const char* jm = getenv("FKADJ_JCACHE")) {
+        const int m = std::atoi(jm);
+        if (m >= 0 && m <= 2) jcache_mode_ = m;
+    }
     tkf_ = 0;
     if (const char* ft = getenv("FKADJ_FUSED_TILE")) {
         const int t = std::atoi(ft);
@@ -926,24 +931,47 @@ fkadj_status Problem::autotune_trials() {
     CK(cudaEventCreate(&a), "event");
     CK(cudaEventCreate(&b), "event");
     const double E = Et_.empty() ? 0.0 : Et_[0];
-    // one warm-up launch, then the best of three rounds of three launches
-    // (a single round mis-ranked presets whose times differ by a few percent)
+    // One warm-up launch, then the best of three rounds of kTrialRun launches.
+    // Where the problem replays its gradients as graphs, a round replays the
+    // launches captured into a graph (programmatic launch off, as in the
+    // gradient's graphs): timed as plain launches, presets within a few
+    // percent of each other were mis-ranked against their replayed times
+    // (64x29 rows of 64x32/640 picked over 64x32/512 at 512x512: 17.6 against
+    // 17.1 us per forward step in the gradient).
+    constexpr int kTrialRun = 6;
     auto timed = [&](auto&& launch, float* ms) -> cudaError_t {
         cudaError_t e = launch();
         if (e) return e;
+        cudaGraphExec_t gx = nullptr;
+        if (graphs_ && !profiling_) {
+            if ((e = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal))) return e;
+            set_launch_pdl(false);
+            cudaError_t le = cudaSuccess;
+            for (int r = 0; r < kTrialRun && !le; ++r) le = launch();
+            set_launch_pdl(true);
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamEndCapture(st_, &graph);
+            if (!e && !le) e = cudaGraphInstantiate(&gx, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (le) e = le;
+            if (e) return e;
+        }
         float best = 1e30f;
-        for (int round = 0; round < 3; ++round) {
-            if ((e = cudaEventRecord(a, st_))) return e;
-            for (int r = 0; r < 3; ++r)
-                if ((e = launch())) return e;
-            if ((e = cudaEventRecord(b, st_))) return e;
-            if ((e = cudaEventSynchronize(b))) return e;
+        for (int round = 0; round < 3 && !e; ++round) {
+            if ((e = cudaEventRecord(a, st_))) break;
+            if (gx) {
+                e = cudaGraphLaunch(gx, st_);
+            } else {
+                for (int r = 0; r < kTrialRun && !e; ++r) e = launch();
+            }
+            if (e || (e = cudaEventRecord(b, st_)) || (e = cudaEventSynchronize(b))) break;
             float t = 0;
-            if ((e = cudaEventElapsedTime(&t, a, b))) return e;
+            if ((e = cudaEventElapsedTime(&t, a, b))) break;
             best = t < best ? t : best;
         }
+        if (gx) cudaGraphExecDestroy(gx);
         *ms = best;
-        return cudaSuccess;
+        return e;
     };
     // every preset at its own height; the forward step and the midpoint also
     // with the rows that fit the grid into one wave of CTAs
@@ -961,7 +989,7 @@ fkadj_status Problem::autotune_trials() {
                 float ms = 0;
                 cudaError_t e = timed([&]() { return make_launch(t, rows[k]); }, &ms);
                 if (e) return e;
-                launches_ += 10;
+                launches_ += 1 + 3 * kTrialRun;
                 if (ms < best) best = ms, tk_[kind] = t, ty_[kind] = rows[k];
             }
         }
@@ -1002,7 +1030,7 @@ fkadj_status Problem::autotune_trials() {
                 return launch_adj_step(tk_[T_ADJ], P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
                                        partial_.as<double>(), nsbx_, st_, fault(), jc, jc + 14 * pl, jc + 7 * pl);
             }, &split_ms);
-        launches_ += 20;
+        launches_ += 2 * (1 + 3 * kTrialRun);
         float fused_best = 1e30f;
         int fused_t = tkf_, fused_p = ADJ_FUSED;
         const bool try_fused = forced_path_ != ADJ_SPLIT;
@@ -1017,7 +1045,7 @@ fkadj_status Problem::autotune_trials() {
                                             gh_.as<double>(), EStep::values(E, E, E), hw_, partial_.as<double>(),
                                             nsbx_, cache ? jc : nullptr, cache ? jc + 7 * pl : nullptr, st_, fault());
                 }, &ms);
-                launches_ += 10;
+                launches_ += 1 + 3 * kTrialRun;
                 if (!e && ms < fused_best) fused_best = ms, fused_t = t, fused_p = path;
             }
         }
@@ -1316,16 +1344,19 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
             have_jcarry = cache;
             return FKADJ_OK;
         }
+        // a null cache makes the step evaluate that Jacobian (the same values)
+        double* jhc = jcache_mode_ >= 2 ? jh : nullptr;
+        const bool carry = jcache_mode_ >= 1;
         CK(prof_begin(K_MID), "profiling event");
         CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), emid(i), hw_, st_, fault(),
                           fin,
-                          fa ? nullptr : fc[nxt], jh, ty_[T_MID], fa),
+                          fa ? nullptr : fc[nxt], jhc, ty_[T_MID], fa),
            "adjoint midpoint");
         CK(prof_end(K_MID), "profiling event");
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
                            gh_.as<double>(), prow(0, i - 1), nsbx_, st_, fault(),
-                           have_jcarry ? jy[cur_c] : nullptr, jh, jy[nxt]),
+                           (carry && have_jcarry) ? jy[cur_c] : nullptr, jhc, carry ? jy[nxt] : nullptr),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
@@ -1333,7 +1364,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         std::swap(z, z2);
         cur_c = nxt;
         have_fcarry = fa == nullptr;
-        have_jcarry = true;
+        have_jcarry = carry;
         return FKADJ_OK;
     };
     if (exact) {

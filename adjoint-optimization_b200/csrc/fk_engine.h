@@ -209,6 +209,10 @@ private:
     int tkf_ = 0;               // fused reference-adjoint preset (fused_shape)
     int adj_path_ = 0;          // AdjPath of the reference-mode backward step
     int forced_path_ = -1;      // AdjPath fixed by FKADJ_ADJ_PATH (-1: autotuned)
+    // Jacobian caches of the split backward step (FKADJ_JCACHE): 2 = J(yh)
+    // from the midpoint kernel and J(y_{i-1}) carried to the next step; 1 =
+    // the carry only, the step evaluates J(yh); 0 = the step evaluates both
+    int jcache_mode_ = 2;
     int ty_[4] = {0, 0, 0, 0};  // rows per tile per kind (0 = the preset's height)
     bool autotune_ = true, tuned_ = false, tuned_fwd_ = false;
     bool own_stream_ = false, have_obj_ = false;
@@ -256,8 +260,8 @@ private:
     GraphKey graph_key(const TrajPlan& tp, bool exact) const;
     int64_t glaunches_ = 0;
     double* gyT_ = nullptr;
-    int buf_gen_ = 0;
-    int pwin_ = 1;               // rows per group in the z.gh partial window            // bumped whenever a buffer the sequence uses is reallocated
+    int buf_gen_ = 0;            // bumped whenever a buffer the sequence uses is reallocated
+    int pwin_ = 1;               // rows per group in the z.gh partial window
     bool capturing_ = false;
     TrajPlan traj_plan_{};
 
