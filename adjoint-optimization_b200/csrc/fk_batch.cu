@@ -683,7 +683,7 @@ fkadj_status BatchEngine::launch_block(int K, const std::vector<int>& ready) {
                         st_),
         "upload block");
     BCK(cudaEventRecord(bev_[r], st_), "block event");
-    const std::pair<int, int> key{K, mask};
+    const std::array<int, 6> key{K, mask, tiles_[0], tiles_[1], tiles_[2], tiles_[3]};
     const BatchInstance* inst = inst_dev_.as<BatchInstance>();
     const BatchItem* dbase = reinterpret_cast<const BatchItem*>(bdev_.as<char>() + block_hdr_bytes());
     const int* dhdr = bdev_.as<int>();

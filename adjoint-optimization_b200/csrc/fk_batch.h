@@ -15,6 +15,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <array>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -129,7 +130,12 @@ private:
     cudaEvent_t bev_[kBlockRing] = {};  // a slot's copy has run
     uint64_t bcount_ = 0;
     DevBuf bdev_;                       // the device block: headers, then items
-    std::vector<std::pair<std::pair<int, int>, cudaGraphExec_t>> bgraphs_;  // (ticks, kind mask) -> graph
+    // (ticks, kind mask, preset of each kind) -> graph: the presets are part of
+    // the key because a graph's launches are fixed at capture, while the
+    // engine cuts its queues into tiles of the current presets (the autotuner
+    // sets them at the first tick with a gradient job, after blocks of
+    // objective-only ticks may have been captured with the default presets)
+    std::vector<std::pair<std::array<int, 6>, cudaGraphExec_t>> bgraphs_;
     static size_t block_hdr_bytes() { return (size_t)kBlockMax * 4 * 4 * sizeof(int); }
     static size_t block_bytes() { return block_hdr_bytes() + sizeof(BatchItem) * (size_t)kBlockMax * 4 * kBatchMaxItems; }
     int device_run(const Job& j) const;  // device actions before the job's next host action

@@ -235,6 +235,85 @@ void Problem::drop_graph() {
     if (gexec_) cudaGraphExecDestroy(gexec_);
     gexec_ = nullptr;
     gkey_ = GraphKey{};
+    drop_segment_graphs();
+}
+
+// ---- segment graphs of a gradient that runs as plain launches
+//
+// A gradient sequence that is not replayed (a configuration's first gradient,
+// and every one-shot call such as the drop-in fkadj_grad) launches the
+// backward sweep's segments of a sqrt store from graphs: each segment (its
+// recompute and its backward steps, about 3 sqrt(nt) launches) is captured
+// while the GPU runs the previous one and launched as one graph, whose
+// kernels follow each other with shorter gaps than plain launches.  Two
+// executable graphs alternate: the one built next is updated in place
+// (cudaGraphExecUpdate, instantiated again when the update is refused) once
+// its previous launch has finished.  Same kernels, same order, same bits.
+// FKADJ_SEGMENT_GRAPHS=0 keeps plain launches.
+void Problem::drop_segment_graphs() {
+    for (int k = 0; k < 2; ++k) {
+        if (seg_exec_[k]) cudaGraphExecDestroy(seg_exec_[k]);
+        seg_exec_[k] = nullptr;
+        if (seg_done_[k]) cudaEventDestroy(seg_done_[k]);
+        seg_done_[k] = nullptr;
+    }
+}
+
+bool Problem::segment_graphs_wanted() const {
+    const char* v = getenv("FKADJ_SEGMENT_GRAPHS");
+    return !(v && v[0] == '0') && graphs_ && !capturing_ && !profiling_;
+}
+
+fkadj_status Problem::segment_begin() {
+    if (!seg_on_) return FKADJ_OK;
+    if (cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();  // this stream cannot be captured: plain launches from here on
+        seg_on_ = false;
+        return FKADJ_OK;
+    }
+    capturing_ = true;
+    set_launch_pdl(false);
+    return FKADJ_OK;
+}
+
+// Ends a segment capture left open by an error return (the stream would stay
+// in capture mode) and switches segment graphs off until the next sequence.
+void Problem::segment_abort() {
+    if (seg_on_ && capturing_) {
+        set_launch_pdl(true);
+        capturing_ = false;
+        cudaGraph_t graph = nullptr;
+        cudaStreamEndCapture(st_, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+    }
+    seg_on_ = false;
+}
+
+fkadj_status Problem::segment_launch() {
+    if (!seg_on_ || !capturing_) return FKADJ_OK;
+    set_launch_pdl(true);
+    capturing_ = false;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st_, &graph);
+    const int k = seg_next_;
+    seg_next_ ^= 1;
+    if (!e && !seg_done_[k]) e = cudaEventCreateWithFlags(&seg_done_[k], cudaEventDisableTiming);
+    if (!e && seg_exec_[k]) {
+        e = cudaEventSynchronize(seg_done_[k]);  // the graph's previous launch has finished
+        cudaGraphExecUpdateResultInfo info;
+        if (!e && cudaGraphExecUpdate(seg_exec_[k], graph, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(seg_exec_[k]);
+            seg_exec_[k] = nullptr;
+        }
+    }
+    if (!e && !seg_exec_[k]) e = cudaGraphInstantiate(&seg_exec_[k], graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (!e) e = cudaGraphLaunch(seg_exec_[k], st_);
+    if (!e) e = cudaEventRecord(seg_done_[k], st_);
+    CK(e, "segment graph");
+    return FKADJ_OK;
 }
 
 fkadj_status Problem::fail_cuda(cudaError_t e, const char* what) {
@@ -381,7 +460,7 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
             }
             if (*q == ',') ++q;
         }
-        if (k == 4) autotune_ = false, tuned_ = true;
+        if (k == 4) autotune_ = false, tuned_ = true, tiles_fixed_ = true;
     }
     subblock_lattice(g_, &nsbx_, &nsby_);
     nsb_ = nsbx_ * nsby_;
@@ -900,6 +979,7 @@ std::map<TuneKey, TuneVal> g_tune;
 }  // namespace
 
 fkadj_status Problem::autotune() {
+    if (tiles_fixed_) return FKADJ_OK;  // the presets FKADJ_TILES gives (the batch engine asks here too)
     const bool want_adjoint = zbuf_.p != nullptr;
     const TuneKey key{device_, g_.nrows, g_.ncols, grad_mode_};
     {
@@ -1015,50 +1095,31 @@ fkadj_status Problem::autotune_trials() {
                 return launch_adj_step(t, P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
                                        partial_.as<double>(), nsbx_, st_, fault(), jc, jc + 14 * pl, jc + 7 * pl);
             });
-        // the fused step against the split pair: every preset, with the J(y)
-        // cache and re-evaluating J(y); trial launches with kept f, as in the
-        // sqrt sweep.  The pair is timed as it runs, midpoint and step launched
-        // in turn (timed one kernel at a time they looked as fast as the fused
-        // step, which ran 6 us slower per backward step in the replayed graph).
-        float split_ms = 0;
-        if (!e)
-            e = timed([&]() {
-                cudaError_t r = launch_adj_mid(tk_[T_MID], P_, g_, y, y, gh_.as<double>(), yh_.as<double>(),
-                                               EStep::values(E, E, E), hw_, st_, fault(), fc, fc + 3 * pl,
-                                               jc + 14 * pl, ty_[T_MID]);
-                if (r) return r;
-                return launch_adj_step(tk_[T_ADJ], P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
-                                       partial_.as<double>(), nsbx_, st_, fault(), jc, jc + 14 * pl, jc + 7 * pl);
-            }, &split_ms);
-        launches_ += 2 * (1 + 3 * kTrialRun);
+        // The fused backward step runs where FKADJ_ADJ_PATH asks for it, its
+        // preset timed here (unless FKADJ_FUSED_TILE fixes it).  The autotuner
+        // does not choose it by itself: in every gradient measured the split
+        // pair was faster (512x512: 36.5 against 42.9 us per backward step;
+        // 2048x2048: 572 against 625 us, 591 re-evaluating J), while trial
+        // launches in isolation, plain or replayed from a graph, timed the
+        // fused step as fast as the pair or faster.
+        const bool try_fused = forced_path_ == ADJ_FUSED || forced_path_ == ADJ_FUSED_RECOMPUTE;
         float fused_best = 1e30f;
-        int fused_t = tkf_, fused_p = ADJ_FUSED;
-        const bool try_fused = forced_path_ != ADJ_SPLIT;
+        int fused_t = tkf_;
         for (int t = 0; !e && try_fused && t < fused_count(); ++t) {
-            if (forced_path_ > 0 && getenv("FKADJ_FUSED_TILE") && t != tkf_) continue;
-            for (int path = ADJ_FUSED; !e && path <= ADJ_FUSED_RECOMPUTE; ++path) {
-                if (forced_path_ > 0 && path != forced_path_) continue;
-                const bool cache = path == ADJ_FUSED;
-                float ms = 0;
-                e = timed([&]() {
-                    return launch_adj_fused(t, P_, g_, y, z2, y, y, fc, fc + 3 * pl, nullptr, wc_.as<uint8_t>(),
-                                            gh_.as<double>(), EStep::values(E, E, E), hw_, partial_.as<double>(),
-                                            nsbx_, cache ? jc : nullptr, cache ? jc + 7 * pl : nullptr, st_, fault());
-                }, &ms);
-                launches_ += 1 + 3 * kTrialRun;
-                if (!e && ms < fused_best) fused_best = ms, fused_t = t, fused_p = path;
-            }
+            if (getenv("FKADJ_FUSED_TILE") && t != tkf_) continue;
+            const bool cache = forced_path_ == ADJ_FUSED;
+            float ms = 0;
+            e = timed([&]() {
+                return launch_adj_fused(t, P_, g_, y, z2, y, y, fc, fc + 3 * pl, nullptr, wc_.as<uint8_t>(),
+                                        gh_.as<double>(), EStep::values(E, E, E), hw_, partial_.as<double>(),
+                                        nsbx_, cache ? jc : nullptr, cache ? jc + 7 * pl : nullptr, st_, fault());
+            }, &ms);
+            launches_ += 1 + 3 * kTrialRun;
+            if (!e && ms < fused_best) fused_best = ms, fused_t = t;
         }
         if (!e) {
-            if (forced_path_ >= 0) {
-                adj_path_ = forced_path_;
-                if (forced_path_ != ADJ_SPLIT) tkf_ = fused_t;
-            } else if (fused_best < split_ms) {
-                adj_path_ = fused_p;
-                tkf_ = fused_t;
-            } else {
-                adj_path_ = ADJ_SPLIT;
-            }
+            adj_path_ = forced_path_ >= 0 ? forced_path_ : ADJ_SPLIT;
+            if (try_fused) tkf_ = fused_t;
         }
     }
     if (!e && zbuf_.p && grad_mode_ == FKADJ_GRAD_EXACT) {
@@ -1247,10 +1308,12 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
             if (t == s0) return slot(k);
             return segslot(t - s0 - 1);
         };
+        if ((s = segment_begin())) return s;
         for (int t = s0; t < s1 - 1; ++t)
             if ((s = step_forward(t, st(t), st(t + 1)))) return s;
         for (int t = s1 - 1; t >= s0; --t)
             if ((s = back(t, st(t)))) return s;
+        if ((s = segment_launch())) return s;
     }
     return FKADJ_OK;
 }
@@ -1293,6 +1356,12 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
     double* yT = cur;
     *yT_out = yT;
     CK(record(ev_[1]), "event");
+    // sqrt-store segments from graphs when this sequence is not itself captured
+    seg_on_ = segment_graphs_wanted();
+    struct SegmentGuard {
+        Problem* p;
+        ~SegmentGuard() { p->segment_abort(); }
+    } seg_guard{this};
     // ---- objective and terminal adjoint state z(T) = -gamma S y(T) (cu-G:1769-1838)
     if ((s = objective_async(yT))) return s;
     CK(cudaMemcpyAsync(hres_, osum_.p, sizeof(double), cudaMemcpyDeviceToHost, st_), "download L0");
@@ -1404,10 +1473,12 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
             auto kept = [&](int t) -> double* {
                 return (tp.keep_f && t >= s0 && t <= s1 - 2) ? fslot(t - s0) : nullptr;
             };
+            if ((s = segment_begin())) return s;
             for (int t = s0; t < s1 - 1; ++t)
                 if ((s = step_forward(t, st(t), st(t + 1), kept(t)))) return s;
             for (int i = s1; i > s0; --i)
                 if ((s = back_step(i, st(i - 1), st(i), kept(i - 1), kept(i)))) return s;
+            if ((s = segment_launch())) return s;
         }
     }
     const int rows = exact ? 3 * nt : nt + 1;

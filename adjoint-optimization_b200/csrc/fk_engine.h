@@ -197,6 +197,16 @@ private:
     // CUDA graph and replayed (use_graph).
     fkadj_status grad_sequence(const TrajPlan& tp, bool exact, double** yT);
     fkadj_status grad_replay(const TrajPlan& tp, bool exact, double** yT);
+    // segment graphs of a gradient run as plain launches (fk_engine.cu)
+    bool segment_graphs_wanted() const;
+    fkadj_status segment_begin();
+    fkadj_status segment_launch();
+    void segment_abort();
+    void drop_segment_graphs();
+    cudaGraphExec_t seg_exec_[2] = {nullptr, nullptr};
+    cudaEvent_t seg_done_[2] = {nullptr, nullptr};
+    int seg_next_ = 0;
+    bool seg_on_ = false;
     void drop_graph();
 
     fkadj_params p_{};
@@ -215,6 +225,7 @@ private:
     int jcache_mode_ = 2;
     int ty_[4] = {0, 0, 0, 0};  // rows per tile per kind (0 = the preset's height)
     bool autotune_ = true, tuned_ = false, tuned_fwd_ = false;
+    bool tiles_fixed_ = false;  // FKADJ_TILES fixed every kind's preset: autotune() keeps them
     bool own_stream_ = false, have_obj_ = false;
     cudaMemPool_t pool_ = nullptr;
     int verbose_ = 0;

@@ -369,7 +369,10 @@ fkadj_status Server::wait(int64_t id, double timeout_s) {
         set_error("timed out waiting for the request");
         return FKADJ_ERR_TIMEOUT;
     }
-    return r->state == 2 ? FKADJ_OK : r->status;
+    if (r->state == 2) return FKADJ_OK;
+    // the failure's message belongs to the thread that ran the request
+    set_error(r->err.empty() ? "request failed" : r->err);
+    return r->status;
 }
 
 fkadj_status Server::result(int64_t id, double* L0, double* LE, double* Lcost, double* gradE, int64_t n,

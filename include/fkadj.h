@@ -169,9 +169,9 @@ void fkadj_problem_last_plan(const fkadj_problem *pb, int64_t out[4]);
  * which launches seven kernels per step, cu-G:1874-1895): out[0] 0 = midpoint
  * and step kernels, 1 = one fused kernel reading the cached J_F(y)^T, 2 = one
  * fused kernel evaluating it; out[1..3] the fused kernel's tile (TX, TY,
- * threads), 0 for the split kernels (fkadj_problem_tiles has theirs).  Chosen
- * by the autotuner at the first gradient unless FKADJ_ADJ_PATH (split, fused,
- * fused-recompute) fixes it. */
+ * threads), 0 for the split kernels (fkadj_problem_tiles has theirs).  The
+ * split kernels run unless FKADJ_ADJ_PATH (fused, fused-recompute) selects the
+ * fused kernel, whose preset the autotuner then times at the first gradient. */
 void fkadj_problem_adjoint_kernel(const fkadj_problem *pb, int out[4]);
 
 /* Sampled per-kernel device time: when enabled, CUDA events bracket about one

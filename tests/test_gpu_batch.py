@@ -108,3 +108,28 @@ def test_batched_fused_adjoint_step_matches_the_split_kernels(monkeypatch, path)
             out[p] = [b.result(j) for j in jobs]
     for a, c in zip(out["split"], out[path]):
         assert np.linalg.norm(c["gradE"] - a["gradE"]) <= 1e-13 * np.linalg.norm(a["gradE"])
+
+
+def test_presets_set_after_objective_only_ticks(monkeypatch):
+    """An objective-only job runs blocks of ticks (replayed from graphs) with
+    the engine's first presets (32x32 tiles) before a gradient job arrives and
+    the presets are set for it (here by FKADJ_TILES, to 16x16 tiles, as the
+    autotuner may do): blocks from then on launch the new presets' kernels,
+    whose tiles the queues are cut into.  Both results equal the one-shot ones."""
+    monkeypatch.setenv("FKADJ_TILES", "4,4,4,4")
+    insts = _mixed(6)
+    obj, grad = insts[2], insts[1]
+    with Batch() as b:
+        po, pg = b.add_problem(obj), b.add_problem(grad)
+        jo = b.submit(po, obj.Et, obj.y0, want_grad=False)
+        b.tick()
+        b.tick()
+        jg = b.submit(pg, grad.Et, grad.y0)
+        b.run()
+        ro, rg = b.result(jo), b.result(jg)
+    g, Lc, L0, LE, _ = api.fk_grad_Et(grad.Et, grad.dt, grad.nt, grad.y0, grad.active_index, grad.ncols,
+                                      grad.nrows, grad.ghost, grad.gamma, grad.S, grad.alpha, params=grad.params)
+    assert abs(rg["Lcost"] - Lc) <= 1e-12 * abs(Lc)
+    assert np.linalg.norm(rg["gradE"] - g) <= 1e-12 * np.linalg.norm(g)
+    ref = api.Problem(obj).objective(obj.Et, obj.y0)
+    assert abs(ro["Lcost"] - ref["Lcost"]) <= 1e-12 * abs(ref["Lcost"])

@@ -56,3 +56,24 @@ def test_profiling_and_graph_runs_agree():
         pb.set_profiling(False)
         c = pb.grad(inst.Et)                      # replay again
     assert np.array_equal(a["gradE"], b["gradE"]) and np.array_equal(a["gradE"], c["gradE"])
+
+
+@pytest.mark.parametrize("mode", [_lib.GRAD_REF, _lib.GRAD_EXACT])
+@pytest.mark.parametrize("nt", [120, 97])
+def test_one_shot_segment_graphs_are_bit_identical(monkeypatch, mode, nt):
+    """A gradient that runs as plain launches (here the drop-in call) launches
+    each segment of its sqrt store from a graph captured while the GPU runs the
+    previous one; the result equals plain launches (FKADJ_SEGMENT_GRAPHS=0)
+    bit for bit, with a short last segment too (nt = 97)."""
+    inst = W.make_instance(64, nt, seed=82, n_obstacles=5, intervals=12, ncols=80,
+                           objective="gradient", alpha=0.1)
+    out = {}
+    for v in ("0", "1"):
+        monkeypatch.setenv("FKADJ_SEGMENT_GRAPHS", v)
+        out[v] = api.fk_grad_Et(inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows,
+                                inst.ghost, inst.gamma, inst.S, inst.alpha, params=inst.params,
+                                opts=api.options(grad_mode=mode, ckpt_policy=_lib.CKPT_SQRT), return_yf=True)
+    a, b = out["0"], out["1"]
+    assert np.array_equal(a[0], b[0])
+    assert a[1] == b[1] and a[2] == b[2]
+    assert np.array_equal(a[5][~np.isnan(a[5])], b[5][~np.isnan(b[5])])

@@ -64,6 +64,32 @@ def test_noalloc_zgh_matches_gradient_entry_point():
             assert abs(got - want) <= 1e-10 * abs(want), (got, want)
 
 
+def test_noalloc_single_row_and_column_grids():
+    """1 x N and N x 1 grids (every sub-block ragged in one direction), after a
+    larger grid so the scratch holds stale partials, against the plain sum of
+    the non-NaN products."""
+    import torch
+    L, fn = _entry()
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(75)
+    d_out = torch.empty(1, dtype=torch.float64, device="cuda")
+    for nr, nc in ((40, 70), (1, 200), (150, 1), (1, 1), (17, 1), (1, 33)):
+        zu = rng.standard_normal(nr * nc)
+        gh = rng.standard_normal(nr * nc)
+        zu[rng.random(nr * nc) < 0.2] = np.nan  # holes
+        t = zu * gh
+        want = float(np.sum(t[~np.isnan(t)]))
+        d_zu = torch.tensor(zu, dtype=torch.float64, device="cuda")
+        d_gh = torch.tensor(gh, dtype=torch.float64, device="cuda")
+        d_out.fill_(float("nan"))
+        rc = fn(d_zu.data_ptr(), d_gh.data_ptr(), nr, nc, d_out.data_ptr(), stream.cuda_stream)
+        assert rc == _lib.OK, L.fkadj_last_error().decode()
+        torch.cuda.synchronize()
+        got = float(d_out.item())
+        scale = float(np.sum(np.abs(t[~np.isnan(t)]))) or 1.0
+        assert abs(got - want) <= 1e-13 * scale, (nr, nc, got, want)
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     import torch
     L, fn = _entry()
