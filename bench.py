@@ -55,7 +55,7 @@ BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
 # dram__bytes_write.sum, caches flushed before the launch) at 512x512.  The reads
 # (33 B/cell: y 24 + gh 8 + halo) reach DRAM; the 24 B/cell of writes stay in the
 # 126 MB L2.
-FWD_TRAFFIC_PER_CELL = 8656640 / 262144
+FWD_TRAFFIC_PER_CELL = 8658176 / 262144
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
 # fused reference-adjoint step (midpoint + four stages in one launch): read z, y_{i-1}, y_i (72) + kept f(y_{i-1}),
 # f(y_i) (48) + gh (8) + weight and stencil codes (2), write z (24); with the J_F(y)^T cache also read J(y_i) and
@@ -65,8 +65,9 @@ FUSED_BYTES_PER_CELL = {"fused": 266.0, "fused-recompute": 154.0}
 # weight code (1); write lambda (24)
 EXACT_BYTES_PER_CELL = 153.0
 # FP64 flops per vector-field evaluation of the forward step (stage update included), counted by ncu
-# (2 x DFMA + DMUL + DADD thread instructions) at 512x512
-FWD_FLOPS_PER_EVAL = 693.6 / 4.58984375
+# (2 x DFMA + DMUL + DADD thread instructions) at 512x512: 692.2 per cell on 64x29 tiles of the
+# 64x32/512 preset, whose launch makes 1216384 evaluations (fwd_evaluations)
+FWD_FLOPS_PER_EVAL = 692.2 * 262144 / 1216384
 
 
 def fwd_evaluations(nrows, ncols, tx, ty):
