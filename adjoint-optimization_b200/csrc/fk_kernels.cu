@@ -65,6 +65,12 @@ constexpr int kLoadUnroll = FKADJ_LOAD_UNROLL;
 #ifndef FKADJ_ADJ_PREFETCH
 #define FKADJ_ADJ_PREFETCH 1
 #endif
+// The same for the single-instance forward step (gh and the step-start
+// state): measured slower (17.3 against 16.3 us at 512^2, 260 against 243 us at
+// 2048^2; 101 registers against 90), so off.
+#ifndef FKADJ_FWD_PREFETCH
+#define FKADJ_FWD_PREFETCH 0
+#endif
 #define FKADJ_BATCH_MINB(tx, ty, nt) (FKADJ_BATCH_ONE_CTA ? 1 : min_blocks(tx, ty, nt))
 
 constexpr int kStageUnroll = FKADJ_STAGE_UNROLL;
@@ -231,7 +237,7 @@ __device__ __forceinline__ void subblock_sums(Term term, double* __restrict__ ro
 //   MODE 2: out = (y0 + D) + cD*k             (last stage, interior only)
 // y0 (the step-start state) comes from global memory; stage algebra and E
 // sources of cu-F:459-562 / cu-F:766-793.
-template <int E, int TX, int TY, int NT, int MODE>
+template <int E, int TX, int TY, int NT, int MODE, bool PF = false>
 __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __restrict__ src,
                                           double* __restrict__ dst, double* __restrict__ D,
                                           const double* __restrict__ y0g, const double* __restrict__ ghs,
@@ -242,23 +248,9 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
     constexpr int W = TX + 2 * E;
     constexpr int IN = TX * TY;
     const int N = W * (rows + 2 * E);
-    RowCol<W, NT> rc(HALO - E, HALO - E);
-#pragma unroll kStageUnroll
-    for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
-        const int r = rc.r, c = rc.c;
-        const int s = r * RW + c;
-        const long long o = (long long)r * ld + c;
-        // global operands first: their latency overlaps the stencil arithmetic; the
-        // first stage's source region is the step-start state itself
-        const double gv = __ldg(ghs + o);
-        double a, b, e;
-        if (MODE == 0) {
-            a = src[s], b = src[RN + s], e = src[2 * RN + s];
-        } else {
-            a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
-        }
-        double ku, kv, kw;
-        rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw, fcs ? (int)__ldg(fcs + o) : -1);
+    // the stage update of cell (r, c) from its step-start value and k
+    auto finish = [&](int r, int c, int s, long long o, double a, double b, double e, double ku, double kv,
+                      double kw) {
         const bool inner = (E == 0) || (r >= HALO && r < HALO + rows && c >= HALO && c < HALO + TX);
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
@@ -292,6 +284,56 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
                 }
             }
         }
+    };
+    RowCol<W, NT> rc(HALO - E, HALO - E);
+    if constexpr (PF) {
+        // Software-pipelined: the next cell's gh and step-start state are
+        // loaded while this cell computes.
+        struct Ops {
+            double gv, a, b, e;
+            int code;
+        };
+        auto fetch = [&](int r, int c, Ops& x) {
+            const long long o = (long long)r * ld + c;
+            x.gv = __ldg(ghs + o);
+            if (MODE != 0) x.a = __ldg(y0g + o), x.b = __ldg(y0g + plane + o), x.e = __ldg(y0g + 2 * plane + o);
+            x.code = fcs ? (int)__ldg(fcs + o) : -1;
+        };
+        Ops cur;
+        if ((int)threadIdx.x < N) fetch(rc.r, rc.c, cur);
+        for (int q = threadIdx.x; q < N; q += NT) {
+            const int r = rc.r, c = rc.c;
+            rc.next();
+            Ops nxt;
+            if (q + NT < N) fetch(rc.r, rc.c, nxt);
+            const int s = r * RW + c;
+            const long long o = (long long)r * ld + c;
+            double a = cur.a, b = cur.b, e = cur.e;
+            if (MODE == 0) a = src[s], b = src[RN + s], e = src[2 * RN + s];
+            double ku, kv, kw;
+            rhs_at<RW, RN>(P, src, s, Ev * cur.gv, ku, kv, kw, cur.code);
+            finish(r, c, s, o, a, b, e, ku, kv, kw);
+            cur = nxt;
+        }
+    } else {
+#pragma unroll kStageUnroll
+        for (int q = threadIdx.x; q < N; q += NT, rc.next()) {
+            const int r = rc.r, c = rc.c;
+            const int s = r * RW + c;
+            const long long o = (long long)r * ld + c;
+            // global operands first: their latency overlaps the stencil arithmetic; the
+            // first stage's source region is the step-start state itself
+            const double gv = __ldg(ghs + o);
+            double a, b, e;
+            if (MODE == 0) {
+                a = src[s], b = src[RN + s], e = src[2 * RN + s];
+            } else {
+                a = __ldg(y0g + o), b = __ldg(y0g + plane + o), e = __ldg(y0g + 2 * plane + o);
+            }
+            double ku, kv, kw;
+            rhs_at<RW, RN>(P, src, s, Ev * gv, ku, kv, kw, fcs ? (int)__ldg(fcs + o) : -1);
+            finish(r, c, s, o, a, b, e, ku, kv, kw);
+        }
     }
     if (MODE != 2) __syncthreads();
 }
@@ -302,7 +344,7 @@ __device__ __forceinline__ void fwd_stage(const DevModel& P, const double* __res
 // are stored there too (three consecutive states), for the discrete-exact
 // adjoint; when `k1` is non-null, k1 = f(y, E0) is stored there (a state).  The tile functions may run several times per CTA (batched
 // kernels): they start by overwriting all the shared memory they read.
-template <int TX, int TY, int NT, bool BULK = false>
+template <int TX, int TY, int NT, bool BULK = false, bool PF = false>
 __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ yin,
                                               double* __restrict__ yout, const double* __restrict__ gh, double E0,
                                               double Eh, double E1, double* __restrict__ stages, int tbx, int tby,
@@ -329,13 +371,13 @@ __device__ __forceinline__ void fwd_step_tile(const DevModel& P, const DevGrid& 
     double* s3 = stages ? stages + sst + off : nullptr;
     double* s4 = stages ? stages + 2 * sst + off : nullptr;
     const uint8_t* fcs = g.fcode ? g.fcode + off : nullptr;
-    fwd_stage<3, TX, TY, NT, 0>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2,
+    fwd_stage<3, TX, TY, NT, 0, PF>(P, A, B, D, y0g, ghs, g.ld, g.plane, E0, dt * 0.5, 1.0 / 6.0 * dt, nullptr, s2,
                                 rows, k1 ? k1 + off : nullptr, fcs);
-    fwd_stage<2, TX, TY, NT, 1>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3,
+    fwd_stage<2, TX, TY, NT, 1, PF>(P, B, A, D, y0g, ghs, g.ld, g.plane, Eh, dt * 0.5, 1.0 / 3.0 * dt, nullptr, s3,
                                 rows, nullptr, fcs);
-    fwd_stage<1, TX, TY, NT, 1>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4,
+    fwd_stage<1, TX, TY, NT, 1, PF>(P, A, B, D, y0g, ghs, g.ld, g.plane, Eh, dt * 1.0, 1.0 / 3.0 * dt, nullptr, s4,
                                 rows, nullptr, fcs);
-    fwd_stage<0, TX, TY, NT, 2>(P, B, A, D, y0g, ghs, g.ld, g.plane, E1, 0.0, dt * 1.0 / 6.0, yout + off, nullptr,
+    fwd_stage<0, TX, TY, NT, 2, PF>(P, B, A, D, y0g, ghs, g.ld, g.plane, E1, 0.0, dt * 1.0 / 6.0, yout + off, nullptr,
                                 rows, nullptr, fcs);
 }
 
@@ -345,8 +387,8 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                const double* __restrict__ gh, EStep E, double* __restrict__ stages, int ty,
                double* __restrict__ k1, unsigned* fault) {
     pdl_enter();
-    fwd_step_tile<TX, TY, NT, true>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages, blockIdx.x, blockIdx.y, ty, k1,
-                                    fault);
+    fwd_step_tile<TX, TY, NT, true, FKADJ_FWD_PREFETCH != 0>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages,
+                                                             blockIdx.x, blockIdx.y, ty, k1, fault);
 }
 
 // ------------------------------------------------- reference-mode adjoint
