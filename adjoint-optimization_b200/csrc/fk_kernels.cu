@@ -629,13 +629,22 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
                 x.j[0] = __ldg(ys + o), x.j[1] = __ldg(ys + g.plane + o), x.j[2] = __ldg(ys + 2 * g.plane + o);
             }
         };
-        Ops cur;
-        if ((int)threadIdx.x < N) fetch(rc.r, rc.c, cur);
+        // FKADJ_ADJ_PREFETCH=2 loads two cells ahead
+        constexpr int DEPTH = FKADJ_ADJ_PREFETCH >= 2 ? 2 : 1;
+        RowCol<W, NT> ahead = rc;  // the cell DEPTH cells after rc's
+        Ops cur, n1;
+        if ((int)threadIdx.x < N) fetch(ahead.r, ahead.c, cur);
+        ahead.next();
+        if constexpr (DEPTH == 2) {
+            if ((int)threadIdx.x + NT < N) fetch(ahead.r, ahead.c, n1);
+            ahead.next();
+        }
         for (int q = threadIdx.x; q < N; q += NT) {
             const int r = rc.r, c = rc.c;
             rc.next();
             Ops nxt;
-            if (q + NT < N) fetch(rc.r, rc.c, nxt);
+            if (q + DEPTH * NT < N) fetch(ahead.r, ahead.c, nxt);
+            ahead.next();
             const int s = r * RW + c;
             const long long o = off + (long long)r * g.ld + c;
             double a = cur.a, b = cur.b, e = cur.e;
@@ -654,7 +663,12 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
                 adj_at<RW, RN>(P, src, s, cur.code, J, ku, kv, kw);
             }
             finish(r, c, s, o, a, b, e, ku, kv, kw);
-            cur = nxt;
+            if constexpr (DEPTH == 2) {
+                cur = n1;
+                n1 = nxt;
+            } else {
+                cur = nxt;
+            }
         }
     } else {
 #pragma unroll kStageUnroll
