@@ -1024,17 +1024,23 @@ fkadj_status Problem::autotune_trials() {
         if (e) return e;
         cudaGraphExec_t gx = nullptr;
         if (graphs_ && !profiling_) {
-            if ((e = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal))) return e;
-            set_launch_pdl(false);
-            cudaError_t le = cudaSuccess;
-            for (int r = 0; r < kTrialRun && !le; ++r) le = launch();
-            set_launch_pdl(true);
-            cudaGraph_t graph = nullptr;
-            e = cudaStreamEndCapture(st_, &graph);
-            if (!e && !le) e = cudaGraphInstantiate(&gx, graph, 0);
-            if (graph) cudaGraphDestroy(graph);
-            if (le) e = le;
-            if (e) return e;
+            if (cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                set_launch_pdl(false);
+                cudaError_t le = cudaSuccess;
+                for (int r = 0; r < kTrialRun && !le; ++r) le = launch();
+                set_launch_pdl(true);
+                cudaGraph_t graph = nullptr;
+                cudaError_t ce = cudaStreamEndCapture(st_, &graph);
+                if (!ce && !le) ce = cudaGraphInstantiate(&gx, graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                if (le) return le;
+                if (ce) {  // the trial graph could not be built: plain launches time the rounds
+                    gx = nullptr;
+                    cudaGetLastError();
+                }
+            } else {
+                cudaGetLastError();  // a stream that cannot be captured: plain launches
+            }
         }
         float best = 1e30f;
         for (int round = 0; round < 3 && !e; ++round) {
