@@ -941,10 +941,20 @@ fkadj_status Problem::ensure_adjoint_work(bool all_rows) {
     // and reduces each block of rows as soon as the backward sweep, which
     // visits rows in decreasing order, has written its lowest one; the batch
     // engine keeps every row.
+    // Under a sqrt store the rows are reduced at the end of each segment
+    // instead (one reduction launch per segment and group, so every segment
+    // has the same launch sequence and its graph can be updated in place,
+    // grad_sequence): the window is then a whole number of segments, so that a
+    // segment's rows never wrap around it.
     const size_t prow = (size_t)(3 * nt_ + 1);
     const int groups = grad_mode_ == FKADJ_GRAD_EXACT ? 3 : 1;
     const int per_group = grad_mode_ == FKADJ_GRAD_EXACT ? nt_ : nt_ + 1;
-    const int win = all_rows ? (int)prow : std::min(per_group, kPartialWindow);
+    int win = std::min(per_group, kPartialWindow);
+    if (traj_plan_.policy == FKADJ_CKPT_SQRT && traj_plan_.stride > 0) {
+        const int c = traj_plan_.stride;
+        win = std::min(per_group, c >= kPartialWindow ? c : c * (kPartialWindow / c));
+    }
+    if (all_rows) win = (int)prow;
     const size_t pbytes = (all_rows ? prow : (size_t)groups * win) * (size_t)nsb_ * sizeof(double);
     if (partial_.bytes < pbytes || pwin_ != win) {
         CK(partial_.alloc(pbytes), "alloc partials");
@@ -1294,7 +1304,9 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
         std::swap(lam, lam2);
-        if (t % pwin_ == 0)  // rows t .. t+pwin-1 of the three groups are complete
+        // rows t .. t+pwin-1 of the three groups are complete (a sqrt store
+        // reduces at the end of each segment instead)
+        if (tp.policy != FKADJ_CKPT_SQRT && t % pwin_ == 0)
             for (int g = 0; g < 3; ++g) CK(flush_rows(g, t, nt), "reduce z.gh");
         return FKADJ_OK;
     };
@@ -1319,6 +1331,7 @@ fkadj_status Problem::grad_exact_backward(const TrajPlan& tp, double* lam, doubl
             if ((s = step_forward(t, st(t), st(t + 1)))) return s;
         for (int t = s1 - 1; t >= s0; --t)
             if ((s = back(t, st(t)))) return s;
+        for (int g = 0; g < 3; ++g) CK(flush_range(g, s0, s1 - s0), "reduce z.gh");
         if ((s = segment_launch())) return s;
     }
     return FKADJ_OK;
@@ -1329,6 +1342,15 @@ cudaError_t Problem::flush_rows(int g, int row, int rows_g) {
     const int n = std::min(pwin_, rows_g - row);
     return launch_sum_rows(partial_.as<double>() + (size_t)g * pwin_ * nsb_, n, nsb_,
                            zgh_.as<double>() + (size_t)g * nt_ + row, st_);
+}
+
+// Reduces rows row0 .. row0+n-1 of group g into zgh; they must not wrap around
+// the window (a sqrt segment's rows, with the window a whole number of
+// segments).
+cudaError_t Problem::flush_range(int g, int row0, int n) {
+    ++launches_;
+    return launch_sum_rows(partial_.as<double>() + ((size_t)g * pwin_ + (size_t)(row0 % pwin_)) * nsb_, n, nsb_,
+                           zgh_.as<double>() + (size_t)g * nt_ + row0, st_);
 }
 
 fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_out) {
@@ -1382,7 +1404,8 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, z, st_), "scatter z");
         CK(launch_dot_gh(g_, z, gh_.as<double>(), prow(0, nt), nsbx_, nsby_, st_), "z.gh");
         launches_ += 2;
-        if (nt % pwin_ == 0) CK(flush_rows(0, nt, nt + 1), "reduce z.gh");
+        if (tp.policy == FKADJ_CKPT_SQRT) CK(flush_range(0, nt, 1), "reduce z.gh");
+        else if (nt % pwin_ == 0) CK(flush_rows(0, nt, nt + 1), "reduce z.gh");
     }
     // ---- backward sweep (cu-G:1866-1908)
     // Work carried from backward step i to step i-1 (computed once, same
@@ -1396,6 +1419,8 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
     // is valid only after a step that evaluated f(y_{i-1}) itself.
     bool have_fcarry = false, have_jcarry = false;
     int cur_c = 0;
+    // a sqrt store reduces its z.gh rows at the end of each segment
+    const bool seg_rows = tp.policy == FKADJ_CKPT_SQRT;
     auto back_step = [&](int i, const double* ya, const double* yb, const double* fa,
                          const double* fb) -> fkadj_status {
         const int nxt = 1 - cur_c;
@@ -1412,7 +1437,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
                "fused adjoint step");
             CK(prof_end(K_ADJ), "profiling event");
             launches_ += 1;
-            if ((i - 1) % pwin_ == 0) CK(flush_rows(0, i - 1, nt + 1), "reduce z.gh");
+            if (!seg_rows && (i - 1) % pwin_ == 0) CK(flush_rows(0, i - 1, nt + 1), "reduce z.gh");
             std::swap(z, z2);
             cur_c = nxt;
             have_fcarry = fa == nullptr;
@@ -1435,7 +1460,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;
-        if ((i - 1) % pwin_ == 0) CK(flush_rows(0, i - 1, nt + 1), "reduce z.gh");
+        if (!seg_rows && (i - 1) % pwin_ == 0) CK(flush_rows(0, i - 1, nt + 1), "reduce z.gh");
         std::swap(z, z2);
         cur_c = nxt;
         have_fcarry = fa == nullptr;
@@ -1484,6 +1509,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
                 if ((s = step_forward(t, st(t), st(t + 1), kept(t)))) return s;
             for (int i = s1; i > s0; --i)
                 if ((s = back_step(i, st(i - 1), st(i), kept(i - 1), kept(i)))) return s;
+            CK(flush_range(0, s0, s1 - s0), "reduce z.gh");  // rows s0 .. s1-1
             if ((s = segment_launch())) return s;
         }
     }

@@ -176,6 +176,7 @@ private:
     }
     // reduces the rows row .. row+pwin-1 (clipped to rows_g) of group g into zgh
     cudaError_t flush_rows(int g, int row, int rows_g);
+    cudaError_t flush_range(int g, int row0, int n);
     static constexpr int kPartialWindow = 512;
     fkadj_status download_grid(const double* d_state, double* host_dense);
     double* slot(int k) const { return traj_.as<double>() + (size_t)k * state_elems(); }
