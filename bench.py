@@ -68,6 +68,10 @@ EXACT_BYTES_PER_CELL = 153.0
 # (2 x DFMA + DMUL + DADD thread instructions) at 512x512: 692.2 per cell on 64x29 tiles of the
 # 64x32/512 preset, whose launch makes 1216384 evaluations (fwd_evaluations)
 FWD_FLOPS_PER_EVAL = 692.2 * 262144 / 1216384
+# the same capture's FP64 pipe activity (sm__pipe_fp64_cycles_active, % of active cycles) and launch duration:
+# DMUL, DADD and compare instructions occupy the pipe as a DFMA does, so the pipe is busier than the flop rate
+# says; scaled to the live launch time it estimates the pipe's activity in the replayed graph
+FWD_FP64_PIPE_NCU = (0.432, 0.020768)  # (fraction, ms of the serialised launch)
 
 
 def fwd_evaluations(nrows, ncols, tx, ty):
@@ -377,6 +381,12 @@ def run_ours(args):
                     "unit": "TFLOP/s", "frac": fl / (fwd_live_ms / 1000.0) / 1e12 / fpeak, "avg_launch_ms": fwd_live_ms,
                     "flops_per_launch": fl, "peak_source": "148 SMs x 64 DFMA/clock x 2 at the sampled SM clock",
                     "flops_source": "ncu-counted FP64 instructions per evaluation at 512x512"}
+    if inst.nrows == 512 and inst.ncols == 512 and (ftx, fty) == (64, 29):
+        frac_ncu, ms_ncu = FWD_FP64_PIPE_NCU
+        roof["fp64"]["pipe_active"] = {
+            "ncu": frac_ncu, "ncu_launch_ms": ms_ncu, "live_estimate": min(1.0, frac_ncu * ms_ncu / fwd_live_ms),
+            "what": "FP64 pipe busy fraction: ncu capture of one serialised launch of the same preset, and that "
+                    "scaled to the live launch time"}
     if roof["traffic"] is None and dom == 0 and FWD_TRAFFIC_PER_CELL:
         roof["traffic"] = FWD_TRAFFIC_PER_CELL * cells
         roof["traffic_source"] = "ncu capture of one k_fwd_step launch at 512x512 (dram read + write)"
