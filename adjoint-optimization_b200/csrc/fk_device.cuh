@@ -81,9 +81,32 @@ struct DevGrid {
 // describes; problems with such cells keep the NaN tests (fcode null).
 constexpr int FC_N = 1, FC_S = 2, FC_W = 4, FC_E = 8, FC_HOLE = 16;
 
+// Refinement of the reciprocal estimate (own_rcp):
+//   0: two Newton-Raphson steps r <- r + r (1 - x r), each squaring the
+//      relative error (4 DFMA);
+//   1: one third-order step r <- r (1 + e + e^2), e = 1 - x r, which cubes it
+//      (3 DFMA): 1/x = r / (1 - e) = r (1 + e + e^2 + e^3 + ...).
+// Both are within one ulp of the quotient; 1 (the default) took the forward
+// step from 16.5 to 16.3 us at 512^2.
+#ifndef FKADJ_RCP_CUBIC
+#define FKADJ_RCP_CUBIC 1
+#endif
+
+// r refined towards 1/x from the estimate r (see FKADJ_RCP_CUBIC)
+__device__ __forceinline__ double rcp_refine(double x, double r) {
+#if FKADJ_RCP_CUBIC
+    const double e = fma(-x, r, 1.0);
+    return fma(r, fma(e, e, e), r);
+#else
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+#endif
+}
+
 // 1/x for positive x or x = +inf without the division's branches: the hardware
-// reciprocal estimate (rcp.approx.ftz.f64) refined by two Newton-Raphson
-// steps r <- r + r (1 - x r), each squaring the relative error.  Within one
+// reciprocal estimate (rcp.approx.ftz.f64) refined by rcp_refine.  Within one
 // ulp of the correctly rounded quotient (tests/test_gpu_mathfn.py); x = +inf,
 // and x beyond 2^1022 (where the estimate flushes the subnormal quotient),
 // give 0.  It takes the three logistic reciprocals and the 1/tau_v- of every
@@ -92,10 +115,7 @@ constexpr int FC_N = 1, FC_S = 2, FC_W = 4, FC_E = 8, FC_HOLE = 16;
 __device__ __forceinline__ double own_rcp(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-    double e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
+    r = rcp_refine(x, r);
     return isinf(x) ? 0.0 : r;  // the refinement turns inf * 0 into NaN
 }
 
@@ -113,12 +133,100 @@ __device__ __forceinline__ double fk_rcp_finite(double x) {
 #if FKADJ_OWN_RCP
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-    double e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-x, r, 1.0);
-    return fma(r, e, r);
+    return rcp_refine(x, r);
 #else
     return 1.0 / x;
+#endif
+}
+
+// The exponential of the smoothed steps (FKADJ_OWN_EXP):
+//   0: CUDA's exp;
+//   1: own, by Cody and Waite's argument reduction (Software Manual for the
+//      Elementary Functions, 1980): x = k ln2 + r with k = rint(x / ln2) and
+//      ln2 split in two so that k ln2_hi is exact, |r| <= ln2 / 2, then e^x =
+//      2^k p(r) with p the degree-11 Chebyshev fit of e^r on [-ln2/2, ln2/2]
+//      (fit error 3.2e-18; coefficients computed with mpmath's chebyfit);
+//   2: own, by Tang's table-driven method (ACM TOMS 15(2), 1989): x =
+//      (16 m + j) ln2/16 + r with |r| <= ln2/32, e^x = 2^m 2^(j/16) (1 + p(r)),
+//      p(r) = r + r^2 q(r) and q the degree-4 Chebyshev fit of
+//      (e^r - 1 - r) / r^2 on [-ln2/32, ln2/32] (error of p 2.8e-17), the 16
+//      values 2^(j/16) in shared memory (exp_table_init).
+// Both own forms are within 1.3 ulp of e^x for x in [-707, 692] (measured
+// against a long-double exp on 2e7 arguments; tests/test_gpu_mathfn.py checks
+// them against CUDA's exp).  They saturate instead of overflowing: for
+// |x| < 2^51 ln2 the result stays in [2^-1020, 2^1000) (k, resp. m, is
+// clamped), so the smoothed steps need no cap of their own.  A NaN argument
+// gives NaN; beyond |x| = 2^51 ln2 (|u| above 1e13, a state that has blown
+// up) and at infinities the value is unspecified.  The rounding to an integer
+// is the fma's own: adding 1.5 * 2^52 leaves rint(x / ln2) in the low bits of
+// the sum.
+// Measured at 512^2 x 2000 steps (sqrt store, one B200): forward step 16.5 us
+// (CUDA's exp), 16.0 (form 1), 15.7 (form 2); 15.4 us with the cubic
+// reciprocal, and the gradient 137.2 -> 132.0 ms.  Form 2 is the default.
+#ifndef FKADJ_OWN_EXP
+#define FKADJ_OWN_EXP 2
+#endif
+
+#if FKADJ_OWN_EXP == 2
+// 2^(j/16), j = 0..15, as the kernels read them (one copy per CTA)
+__shared__ double fk_exp2_tab[16];
+__constant__ double kExp2Tab[16] = {
+    0x1.0000000000000p+0, 0x1.0b5586cf9890fp+0, 0x1.172b83c7d517bp+0, 0x1.2387a6e756238p+0,
+    0x1.306fe0a31b715p+0, 0x1.3dea64c123422p+0, 0x1.4bfdad5362a27p+0, 0x1.5ab07dd485429p+0,
+    0x1.6a09e667f3bcdp+0, 0x1.7a11473eb0187p+0, 0x1.8ace5422aa0dbp+0, 0x1.9c49182a3f090p+0,
+    0x1.ae89f995ad3adp+0, 0x1.c199bdd85529cp+0, 0x1.d5818dcfba487p+0, 0x1.ea4afa2a490dap+0};
+#endif
+
+// Every kernel that evaluates the model calls this before its first CTA
+// barrier (the table form fills its shared table; the others do nothing).
+__device__ __forceinline__ void exp_table_init() {
+#if FKADJ_OWN_EXP == 2
+    if (threadIdx.x < 16) fk_exp2_tab[threadIdx.x] = kExp2Tab[threadIdx.x];
+#endif
+}
+
+__device__ __forceinline__ double fk_exp(double x) {
+#if FKADJ_OWN_EXP == 1
+    constexpr double kShift = 0x1.8p52;
+    const double t = fma(x, 0x1.71547652b82fep+0, kShift);  // 1.5 2^52 + rint(x / ln2)
+    const double kd = t - kShift;
+    int k = __double2loint(t);
+    double r = fma(kd, -0x1.62e42fefa3800p-1, x);  // exact: ln2_hi has 42 significant bits
+    r = fma(kd, -0x1.ef35793c76730p-45, r);
+    double p = 0x1.af631d0059becp-26;
+    p = fma(p, r, 0x1.28b4057f44145p-22);
+    p = fma(p, r, 0x1.71ddf5749d126p-19);
+    p = fma(p, r, 0x1.a01991ac8730ap-16);
+    p = fma(p, r, 0x1.a01a01b14378fp-13);
+    p = fma(p, r, 0x1.6c16c187fbe02p-10);
+    p = fma(p, r, 0x1.111111110f225p-7);
+    p = fma(p, r, 0x1.555555554f0cfp-5);
+    p = fma(p, r, 0x1.555555555555ap-3);
+    p = fma(p, r, 0x1.0000000000011p-1);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    k = min(max(k, -1020), 999);
+    return p * __hiloint2double((k + 1023) << 20, 0);  // times 2^k, exactly
+#elif FKADJ_OWN_EXP == 2
+    constexpr double kShift = 0x1.8p52;
+    const double t = fma(x, 0x1.71547652b82fep+4, kShift);  // 1.5 2^52 + rint(16 x / ln2)
+    const double kd = t - kShift;
+    const int k = __double2loint(t);
+    double r = fma(kd, -0x1.62e42fefa0000p-5, x);  // exact: (ln2/16)_hi has 36 significant bits
+    r = fma(kd, -0x1.cf79abc9e3b3ap-44, r);
+    double q = 0x1.6c17bb51f236dp-10;
+    q = fma(q, r, 0x1.11120af701debp-7);
+    q = fma(q, r, 0x1.55555555194d2p-5);
+    q = fma(q, r, 0x1.55555554dd44dp-3);
+    q = fma(q, r, 0.5);
+    const double pm1 = fma(r * r, q, r);  // e^r - 1
+    const int m = min(max(k >> 4, -1020), 998);  // k >> 4 = floor(k / 16)
+    const double T = fk_exp2_tab[k & 15];
+    // 2^m 2^(j/16): m added to the exponent field (T in [1, 2), m clamped)
+    const double Ts = __hiloint2double(__double2hiint(T) + (m << 20), __double2loint(T));
+    return fma(Ts, pm1, Ts);
+#else
+    return exp(x);
 #endif
 }
 
@@ -137,7 +245,9 @@ struct Step {
 // above it s is 2^-1000 instead of 0 and 1 - s is 1.
 __device__ __forceinline__ Step step_of_exp(double e) {
 #if FKADJ_FAST_STEPS
-    e = fmin(e, 0x1p1000);
+#if FKADJ_OWN_EXP == 0
+    e = fmin(e, 0x1p1000);  // the own exponentials stay below 2^1000 by themselves
+#endif
     const double s = fk_rcp_finite(1.0 + e);
     return {s, e * s};
 #else
@@ -146,14 +256,14 @@ __device__ __forceinline__ Step step_of_exp(double e) {
     return {s, s == 0.0 ? 1.0 : e * s};
 #endif
 }
-__device__ __forceinline__ Step smooth_step(double x) { return step_of_exp(exp(-2.0 * x)); }
+__device__ __forceinline__ Step smooth_step(double x) { return step_of_exp(fk_exp(-2.0 * x)); }
 
 // e^{-2 k (u - u0)} as the smoothed steps take it; m2k = -2 k (the same product)
 __device__ __forceinline__ double step_exp(double m2k, double k, double u, double u0) {
 #if FKADJ_FAST_STEPS
-    return exp(m2k * (u - u0));
+    return fk_exp(m2k * (u - u0));
 #else
-    return exp(-2.0 * (k * (u - u0)));
+    return fk_exp(-2.0 * (k * (u - u0)));
 #endif
 }
 
@@ -161,7 +271,7 @@ __device__ __forceinline__ double step_exp(double m2k, double k, double u, doubl
 // one exp for both.
 __device__ __forceinline__ void steps_pq(const DevModel& P, double u, Step& sp, Step& sq) {
 #if FKADJ_SHARED_EXP
-    const double e = exp(-2.0 * (P.ksm * (u - P.u_c)));
+    const double e = fk_exp(-2.0 * (P.ksm * (u - P.u_c)));
     sp = step_of_exp(e);
     sq = step_of_exp(e * P.eq);
 #else
@@ -270,6 +380,25 @@ __device__ __forceinline__ double finite_u(double u) {
 #endif
 }
 
+// NaN tests of the forward stencil (the hole test and the four mirrored
+// neighbours): FP64 compares (0), or integer tests of the high word (1), which
+// keep them off the FP64 pipe.  The integer test sees every NaN whose
+// significand has a bit set in its high word, i.e. every NaN arithmetic or the
+// NaN ring produces (quiet NaNs); a signalling NaN with only low-word payload
+// bits would pass for an infinity, and none is ever stored.  Measured slower
+// (forward step 15.6 against 15.4 us at 512^2: the integer tests take more
+// issue slots than the compares take FP64 cycles), so off.
+#ifndef FKADJ_INT_NAN
+#define FKADJ_INT_NAN 0
+#endif
+__device__ __forceinline__ bool stencil_nan(double x) {
+#if FKADJ_INT_NAN
+    return ((unsigned)__double2hiint(x) << 1) > 0xffe00000u;
+#else
+    return isnan(x);
+#endif
+}
+
 // Forward stencil codes (FC_*) in place of the NaN tests: measured slower on
 // B200 (forward step 18.3 against 17.0 us at 512^2), so off by default.
 #ifndef FKADJ_FWD_CODES
@@ -307,15 +436,15 @@ __device__ __forceinline__ void rhs_at(const DevModel& P, const double* __restri
 #endif
 #if FKADJ_HOLE_BRANCH
     // holes and the NaN ring skip the arithmetic (their result is NaN either way)
-    if (isnan(u)) {
+    if (stencil_nan(u)) {
         fu = fv = fw = u;
         return;
     }
 #endif
     const double v = Y[RN + q], w = Y[2 * RN + q];
     const double un = Y[q - W], us = Y[q + W], uw = Y[q - 1], ue = Y[q + 1];
-    const bool nN = isnan(un), nS = !nN && isnan(us);
-    const bool nW = isnan(uw), nE = !nW && isnan(ue);
+    const bool nN = stencil_nan(un), nS = !nN && stencil_nan(us);
+    const bool nW = stencil_nan(uw), nE = !nW && stencil_nan(ue);
 #if FKADJ_MIRROR_OFFSETS
     // the same neighbours as the selects below, read where they are
     const int qa = nN ? q + W : q - W, qb = nS ? q - W : q + W;

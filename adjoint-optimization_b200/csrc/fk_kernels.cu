@@ -387,6 +387,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                const double* __restrict__ gh, EStep E, double* __restrict__ stages, int ty,
                double* __restrict__ k1, unsigned* fault) {
     pdl_enter();
+    exp_table_init();
     fwd_step_tile<TX, TY, NT, true, FKADJ_FWD_PREFETCH != 0>(P, g, yin, yout, gh, E.a(), E.b(), E.c(), stages,
                                                              blockIdx.x, blockIdx.y, ty, k1, fault);
 }
@@ -556,6 +557,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
               const double* __restrict__ fin, double* __restrict__ fout, double* __restrict__ jh, int ty,
               const double* __restrict__ fa, unsigned* fault) {
     pdl_enter();
+    exp_table_init();
     adj_mid_tile<TX, TY, NT, true, FKADJ_ADJ_PREFETCH != 0>(P, g, ya, yb, gh, yh, E.a(), E.b(), E.c(), hw, fin, fout,
                                                             jh, blockIdx.x, blockIdx.y, ty, fa, fault);
 }
@@ -749,6 +751,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja,
                unsigned* fault) {
     pdl_enter();
+    exp_table_init();
     adj_step_tile<TX, TY, NT, true, FKADJ_ADJ_PREFETCH != 0>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh,
                                                              ja, blockIdx.x, blockIdx.y, fault);
 }
@@ -962,6 +965,7 @@ __global__ void __launch_bounds__(NT, 1)
                 const double* __restrict__ gh, EStep E, HermiteW hw, double* __restrict__ row, int nsbx,
                 const double* __restrict__ jb, double* __restrict__ ja, unsigned* fault) {
     pdl_enter();
+    exp_table_init();
     adj_fused_tile<TX, TY, NT>(P, g, z, zout, ya, yb, fa, fb, fout, wc, gh, E.a(), E.b(), E.c(), hw, row, nsbx, jb,
                                ja, blockIdx.x, blockIdx.y, fault);
 }
@@ -1129,6 +1133,7 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                 const double* __restrict__ gh, double* __restrict__ r1, double* __restrict__ r23,
                 double* __restrict__ r4, int nsbx, unsigned* fault) {
     pdl_enter();
+    exp_table_init();
     adj_exact_tile<TX, TY, NT, true, FKADJ_ADJ_PREFETCH != 0>(P, g, lam, lamout, y, stages, wc, gh, r1, r23, r4, nsbx,
                                                               blockIdx.x, blockIdx.y, fault);
 }
@@ -1176,6 +1181,7 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_fwd(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
+    exp_table_init();
     uint32_t phase = 0;  // bulk transfers of this CTA so far (the tile-copy barrier's phase)
     const QueueView q(t);
     for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {
@@ -1192,6 +1198,7 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_mid(const BatchInstance* __restrict__ inst, const BatchQueue t, HermiteW hw) {
     pdl_enter();
+    exp_table_init();
     uint32_t phase = 0;
     const QueueView q(t);
     for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {
@@ -1208,6 +1215,7 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, FKADJ_BATCH_MINB(TX, TY, NT))
     k_batch_adj(const BatchInstance* __restrict__ inst, const BatchQueue t) {
     pdl_enter();
+    exp_table_init();
     uint32_t phase = 0;
     const QueueView q(t);
     for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {
@@ -1228,6 +1236,7 @@ template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 1) k_batch_fused(const BatchInstance* __restrict__ inst, const BatchQueue t,
                                                        HermiteW hw) {
     pdl_enter();
+    exp_table_init();
     uint32_t phase = 0;
     const QueueView q(t);
     for (int tile = blockIdx.x; tile < q.tiles; tile += gridDim.x) {

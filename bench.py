@@ -55,7 +55,7 @@ BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
 # dram__bytes_write.sum, caches flushed before the launch) at 512x512.  The reads
 # (33 B/cell: y 24 + gh 8 + halo) reach DRAM; the 24 B/cell of writes stay in the
 # 126 MB L2.
-FWD_TRAFFIC_PER_CELL = 8658176 / 262144
+FWD_TRAFFIC_PER_CELL = 8654848 / 262144
 KERNEL_NAMES = {0: "k_fwd_step", 1: "k_adj_mid", 2: "k_adj_step"}
 # fused reference-adjoint step (midpoint + four stages in one launch): read z, y_{i-1}, y_i (72) + kept f(y_{i-1}),
 # f(y_i) (48) + gh (8) + weight and stencil codes (2), write z (24); with the J_F(y)^T cache also read J(y_i) and
@@ -65,13 +65,13 @@ FUSED_BYTES_PER_CELL = {"fused": 266.0, "fused-recompute": 154.0}
 # weight code (1); write lambda (24)
 EXACT_BYTES_PER_CELL = 153.0
 # FP64 flops per vector-field evaluation of the forward step (stage update included), counted by ncu
-# (2 x DFMA + DMUL + DADD thread instructions) at 512x512: 692.2 per cell on 64x29 tiles of the
-# 64x32/512 preset, whose launch makes 1216384 evaluations (fwd_evaluations)
-FWD_FLOPS_PER_EVAL = 692.2 * 262144 / 1216384
+# (2 x DFMA + DMUL + DADD thread instructions) at 512x512: 585.1 per cell on 64x29 tiles of the
+# 64x32/640 preset, whose launch makes 1216384 evaluations (fwd_evaluations)
+FWD_FLOPS_PER_EVAL = 585.1 * 262144 / 1216384
 # the same capture's FP64 pipe activity (sm__pipe_fp64_cycles_active, % of active cycles) and launch duration:
 # DMUL, DADD and compare instructions occupy the pipe as a DFMA does, so the pipe is busier than the flop rate
 # says; scaled to the live launch time it estimates the pipe's activity in the replayed graph
-FWD_FP64_PIPE_NCU = (0.432, 0.020768)  # (fraction, ms of the serialised launch)
+FWD_FP64_PIPE_NCU = (0.400, 0.019936)  # (fraction, ms of the serialised launch)
 
 
 def fwd_evaluations(nrows, ncols, tx, ty):
@@ -369,9 +369,10 @@ def run_ours(args):
             "tiles": {k: list(v) for k, v in tiles.items()
                       if (k == "adj_exact") == (args.mode == "exact") or k == "fwd_step"},
             "adjoint_path": pb.adjoint_kernel,
-            "note": "FP64 bound: a vector-field evaluation costs 2 exp, 4 reciprocals and ~60 "
-                    "FMA-class operations, 4.6 evaluations per cell-step; the HBM fraction is reported "
-                    "against the copy peak"}
+            "note": "FP64 bound: a vector-field evaluation costs 2 exp (table-driven, 11 FP64 "
+                    "instructions each), 4 reciprocals (estimate + one cubic refinement) and ~50 "
+                    "FMA-class operations, 126 FP64 flops, 4.6 evaluations per cell-step; the HBM fraction "
+                    "is reported against the copy peak"}
     # the forward step against the FP64 roof (the bound it is nearer to)
     ftx, fty, _ = tiles["fwd_step"]
     fl = FWD_FLOPS_PER_EVAL * fwd_evaluations(inst.nrows, inst.ncols, ftx, fty)

@@ -1,9 +1,16 @@
-"""The kernels' own reciprocal (fk_device.cuh `own_rcp`: the hardware estimate
-refined by two Newton-Raphson steps, in place of the IEEE division) against the
-correctly rounded quotient: within one ulp over the denominators the model
-produces (1 + e^{...} from 1 to 1e300, the tau_v- range), exact at powers of
-two, 0 at +inf and beyond 2^1022.  The probe source is compiled here for sm_100a;
-the build check runs without a GPU."""
+"""The kernels' own math functions on the GPU.
+
+Reciprocal (fk_device.cuh `own_rcp`: the hardware estimate refined without a
+division, by either refinement FKADJ_RCP_CUBIC selects) against the correctly rounded quotient: within one ulp over the
+denominators the model produces (1 + e^{...} from 1 to 1e300, the tau_v-
+range), exact at powers of two, 0 at +inf and beyond 2^1022.
+
+Exponential (`fk_exp`, each form FKADJ_OWN_EXP selects) against CUDA's exp:
+within 3 ulp (each within about one ulp of e^x) over the arguments the smoothed steps see and far beyond them,
+NaN for NaN, and saturated (never inf, never 0) at the ends of the range.
+
+The probe source is compiled here for sm_100a; the build check runs without a
+GPU."""
 import ctypes
 import os
 import shutil
@@ -23,9 +30,9 @@ def _nvcc():
     pytest.skip("nvcc not found")
 
 
-def _build(out):
+def _build(out, defs=()):
     cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-           "-shared", "-o", out, PROBE]
+           *defs, "-shared", "-o", out, PROBE]
     subprocess.run(cmd, check=True, capture_output=True, timeout=600)
     return out
 
@@ -44,8 +51,9 @@ def _inputs():
 
 
 @pytest.mark.gpu
-def test_own_reciprocal_within_one_ulp(tmp_path):
-    lib = ctypes.CDLL(_build(str(tmp_path / "probe.so")))
+@pytest.mark.parametrize("cubic", [0, 1])
+def test_own_reciprocal_within_one_ulp(tmp_path, cubic):
+    lib = ctypes.CDLL(_build(str(tmp_path / f"probe_rcp{cubic}.so"), (f"-DFKADJ_RCP_CUBIC={cubic}",)))
     lib.probe_rcp.restype = ctypes.c_int
     lib.probe_rcp.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_longlong]
 
@@ -65,5 +73,33 @@ def test_own_reciprocal_within_one_ulp(tmp_path):
     np.testing.assert_array_equal(own_p2, 1.0 / p2)       # exact at powers of two
     big, _ = run(np.array([np.ldexp(1.5, 1022), 1.7e308, np.inf]))  # quotients below 2^-1022 flush to 0
     assert np.all(big == 0.0)                             # the logistic then takes s = 0, 1 - s = 1
+    nan, _ = run(np.array([np.nan]))
+    assert np.isnan(nan[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", [1, 2])
+def test_own_exponential_within_three_ulp_of_cuda_exp(tmp_path, form):
+    lib = ctypes.CDLL(_build(str(tmp_path / f"probe_exp{form}.so"), (f"-DFKADJ_OWN_EXP={form}",)))
+    lib.probe_exp.restype = ctypes.c_int
+    lib.probe_exp.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_longlong]
+
+    def run(x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        own, ref = np.empty_like(x), np.empty_like(x)
+        assert lib.probe_exp(x.ctypes.data, own.ctypes.data, ref.ctypes.data, x.size) == 0
+        return own, ref
+
+    rng = np.random.default_rng(12)
+    # -2 ksm (u - u_c) and -2 k_fk (u - u_csi) for u in [-1, 2], then the whole normal range
+    x = np.concatenate([rng.uniform(-400.0, 250.0, 600_000), rng.uniform(-40.0, 40.0, 200_000),
+                        rng.uniform(-707.0, 692.0, 200_000), rng.uniform(-1e-3, 1e-3, 50_000),
+                        np.arange(-2040, 1996) * (np.log(2.0) / 4.0),  # about the reduction's breakpoints
+                        [0.0, -0.0, 1.0, -1.0, 1e-300]])
+    own, ref = run(x)
+    ulps = np.abs(own.view(np.int64) - ref.view(np.int64))
+    assert ulps.max() <= 3, f"max {ulps.max()} ulp at x={x[ulps.argmax()]!r}"
+    edge, _ = run(np.array([693.0, 710.0, 1e4, 1e12, -710.0, -1e4, -1e12]))
+    assert np.all(np.isfinite(edge)) and np.all(edge > 0) and np.all(edge < 2.0 ** 1000)
     nan, _ = run(np.array([np.nan]))
     assert np.isnan(nan[0])
