@@ -55,6 +55,9 @@ static DevModel make_model(const fkadj_params& p, double dt) {
     M.cv = p.Dv / (p.h * p.h);
     M.cw = p.Dw / (p.h * p.h);
     M.dt = dt;
+    M.two_ksm = 2.0 * p.ksm;
+    M.kfk_r2tsi = p.k_fk / (2 * p.tau_si);
+    M.hksm_dv12 = 0.5 * p.ksm * M.dv12;
     return M;
 }
 
@@ -1114,10 +1117,11 @@ fkadj_status Problem::autotune_trials() {
         // The fused backward step runs where FKADJ_ADJ_PATH asks for it, its
         // preset timed here (unless FKADJ_FUSED_TILE fixes it).  The autotuner
         // does not choose it by itself: in every gradient measured the split
-        // pair was faster (512x512: 36.5 against 42.9 us per backward step;
-        // 2048x2048: 572 against 625 us, 591 re-evaluating J), while trial
-        // launches in isolation, plain or replayed from a graph, timed the
-        // fused step as fast as the pair or faster.
+        // pair was faster or as fast (512x512: 34.5 against 40.2 us per
+        // backward step, 38.1 re-evaluating J; 2048x2048: 450 against 492 us,
+        // 446 re-evaluating J), while trial launches in isolation, plain or
+        // replayed from a graph, timed the fused step as fast as the pair or
+        // faster.
         const bool try_fused = forced_path_ == ADJ_FUSED || forced_path_ == ADJ_FUSED_RECOMPUTE;
         float fused_best = 1e30f;
         int fused_t = tkf_;
@@ -1448,7 +1452,8 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         double* jhc = jcache_mode_ >= 2 ? jh : nullptr;
         const bool carry = jcache_mode_ >= 1;
         CK(prof_begin(K_MID), "profiling event");
-        CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), yh_.as<double>(), emid(i), hw_, st_, fault(),
+        CK(launch_adj_mid(tk_[T_MID], P_, g_, ya, yb, gh_.as<double>(), jhc ? nullptr : yh_.as<double>(), emid(i),
+                          hw_, st_, fault(),
                           fin,
                           fa ? nullptr : fc[nxt], jhc, ty_[T_MID], fa),
            "adjoint midpoint");

@@ -425,7 +425,9 @@ __device__ __forceinline__ void store_jac(double* __restrict__ Jb, long long pla
 //   read from there instead of evaluated, and f(ya, Ea) goes to fout;
 //   f(ya, Ea) is k1 of the forward step from ya: when fa is non-null (the
 //   forward recompute kept it) it is read from there too;
-//   J_F(yh)^T, used by stages 2 and 3 of the adjoint step, goes to jh.
+//   J_F(yh)^T, used by stages 2 and 3 of the adjoint step, goes to jh; yh
+//   itself is stored only where yh is non-null (a step that reads the J(yh)
+//   cache never reads yh).
 template <int TX, int TY, int NT, bool BULK = false, bool PF = false>
 __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g, const double* __restrict__ ya,
                                              const double* __restrict__ yb, const double* __restrict__ gh,
@@ -541,9 +543,8 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
             rhs_at<RW, RN>(P, C, s, E3 * __ldg(gh + o), m2[0], m2[1], m2[2], g.fcode ? (int)__ldg(g.fcode + o) : -1);
 #pragma unroll
             for (int f = 0; f < 3; ++f) {
-                double* p = yh + o + f * g.plane;
                 yv[f] = Q[f * TX * TY + (r - H2) * TX + (c - H2)] + hw.c2 * (m2[f] * dt);
-                *p = yv[f];
+                if (yh) yh[o + f * g.plane] = yv[f];
             }
             if (jh && !isnan(yv[0])) store_jac(jh, g.plane, o, fk_jacT(P, yv[0], yv[1], yv[2]));
         }

@@ -47,8 +47,8 @@ UNIT = "gradients/s"
 
 # bytes per dense cell per launch the kernels move as designed (one RK4 step)
 BYTES_PER_CELL = {0: 56.0,    # forward step: read y (24) + gh (8), write y (24)
-                  1: 184.0,   # adjoint midpoint: read y_{i-1}, y_i (48) + f(y_{i-1}), f(y_i) (48) + gh (8),
-                              #   write yh (24) + J(yh) (56)
+                  1: 160.0,   # adjoint midpoint: read y_{i-1}, y_i (48) + f(y_{i-1}), f(y_i) (48) + gh (8),
+                              #   write J(yh) (56; yh itself is not stored while the J(yh) cache is read)
                   2: 249.0}   # adjoint step: read z (24) + J(y_i), J(yh) (112) + y_{i-1} (24) + gh (8)
                               #   + weight code (1), write z (24) + J(y_{i-1}) (56)
 # DRAM bytes per cell of one k_fwd_step launch measured by ncu (dram__bytes_read.sum +
