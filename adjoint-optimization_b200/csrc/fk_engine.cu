@@ -458,7 +458,7 @@ fkadj_status Problem::init(const fkadj_params& p, double dt, int nt, const int* 
             q = end;
             if (*q == ':') {
                 const long r = std::strtol(q + 1, &end, 10);
-                if (r > 0 && r <= tile_shape((int)t).ty && (k == T_FWD || k == T_MID)) ty_[k] = (int)r;
+                if (r > 0 && r <= tile_shape((int)t).ty && (k == T_FWD || k == T_MID || k == T_ADJ)) ty_[k] = (int)r;
                 q = end;
             }
             if (*q == ',') ++q;
@@ -952,19 +952,50 @@ fkadj_status Problem::ensure_adjoint_work(bool all_rows) {
     const size_t prow = (size_t)(3 * nt_ + 1);
     const int groups = grad_mode_ == FKADJ_GRAD_EXACT ? 3 : 1;
     const int per_group = grad_mode_ == FKADJ_GRAD_EXACT ? nt_ : nt_ + 1;
+    const bool sqrt_store = traj_plan_.policy == FKADJ_CKPT_SQRT && traj_plan_.stride > 0;
     int win = std::min(per_group, kPartialWindow);
-    if (traj_plan_.policy == FKADJ_CKPT_SQRT && traj_plan_.stride > 0) {
+    if (sqrt_store) {
         const int c = traj_plan_.stride;
         win = std::min(per_group, c >= kPartialWindow ? c : c * (kPartialWindow / c));
     }
+    // Lattice of the partials.  Row segments (16 times as many partials as
+    // 16x16 sub-blocks) where the reference-mode split step reduces windowed
+    // partials, the window shrunk, in whole segments under a sqrt store, until
+    // it holds no more than the full rows of 16x16 partials that
+    // estimate_bytes counts; the 16x16 lattice for the exact mode, the fused
+    // step, the batch engine's all-rows buffers, where no window fits, or under
+    // FKADJ_ZGH_SEGMENTS=0.
+    // The choice depends on the grid, the horizon and the device only, never on
+    // the store, so that every store gives the same bits: row segments need
+    // room for one segment of rows of the sqrt store (whichever store runs),
+    // and pay only where 64x32 tiles fit the grid into one wave of CTAs, one
+    // per SM (512 x 512 and below): there tiles of any height make the wave
+    // full (512^2 x 2000 gradient 132.0 -> 129.4 ms), while at 2048 x 2048,
+    // 14 waves, the 16-fold partials cost 1.4 %.
+    const size_t nsb16 = (size_t)nsbx_ * (size_t)nsby_, nsbseg = (size_t)nsbx_ * (size_t)g_.nrows;
+    const size_t fit = prow * (nsb16 + 1) / nsbseg;  // rows of segment partials within that count
+    const int c_sqrt = std::max(2, (int)std::ceil(std::sqrt((double)nt_)));  // plan_trajectory's stride
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_) != cudaSuccess) sms = 0;
+    const bool one_wave = (int64_t)((g_.nrows + 31) / 32) * ((g_.ncols + 63) / 64) <= (int64_t)sms;
+    bool segs = !all_rows && grad_mode_ == FKADJ_GRAD_REF && (forced_path_ < 0 || forced_path_ == ADJ_SPLIT) &&
+                one_wave && fit >= (size_t)std::min(per_group, c_sqrt);
+    if (const char* sv = getenv("FKADJ_ZGH_SEGMENTS")) segs = segs && std::atoi(sv) != 0;
+    if (segs && (size_t)win > fit) {
+        const int c = sqrt_store ? traj_plan_.stride : 1;
+        win = (int)std::max<size_t>(std::min<size_t>((size_t)win, fit / (size_t)c * (size_t)c), (size_t)c);
+    }
     if (all_rows) win = (int)prow;
-    const size_t pbytes = (all_rows ? prow : (size_t)groups * win) * (size_t)nsb_ * sizeof(double);
-    if (partial_.bytes < pbytes || pwin_ != win) {
+    const size_t nsb = segs ? nsbseg : nsb16;
+    const size_t pbytes = (all_rows ? prow : (size_t)groups * win) * nsb * sizeof(double);
+    if (partial_.bytes < pbytes || pwin_ != win || segs_ != segs) {
         CK(partial_.alloc(pbytes), "alloc partials");
         CK(cudaMemsetAsync(partial_.p, 0, partial_.bytes, st_), "zero partials");
         pwin_ = win;
         ++buf_gen_;
     }
+    segs_ = segs;
+    nsb_ = (int)nsb;
     if (zgh_.bytes < prow * sizeof(double)) {
         CK(zgh_.alloc(prow * sizeof(double)), "alloc zgh");
         ++buf_gen_;
@@ -1080,8 +1111,8 @@ fkadj_status Problem::autotune_trials() {
         best = 1e30f;
         for (int t = 0; t < tile_count(); ++t) {
             int rows[2] = {0, 0}, nr = 1;  // 0 = the preset's height
-            if (kind == T_FWD || kind == T_MID) {
-                const int bal = balanced_rows(t, kind == T_FWD ? 0 : 1, g_);
+            if (kind == T_FWD || kind == T_MID || (kind == T_ADJ && segs_)) {
+                const int bal = balanced_rows(t, kind == T_FWD ? 0 : (kind == T_MID ? 1 : 2), g_);
                 if (bal > 0 && bal < tile_shape(t).ty) rows[nr++] = bal;
             }
             for (int k = 0; k < nr; ++k) {
@@ -1110,9 +1141,10 @@ fkadj_status Problem::autotune_trials() {
                                   fc + 3 * pl, jc + 14 * pl, ty);
         });
         if (!e)
-            e = pick(T_ADJ, [&](int t, int) {
+            e = pick(T_ADJ, [&](int t, int ty) {
                 return launch_adj_step(t, P_, g_, y, z2, y, y, y, wc_.as<uint8_t>(), gh_.as<double>(),
-                                       partial_.as<double>(), nsbx_, st_, fault(), jc, jc + 14 * pl, jc + 7 * pl);
+                                       partial_.as<double>(), nsbx_, st_, fault(), jc, jc + 14 * pl, jc + 7 * pl, ty,
+                                       segs_);
             });
         // The fused backward step runs where FKADJ_ADJ_PATH asks for it, its
         // preset timed here (unless FKADJ_FUSED_TILE fixes it).  The autotuner
@@ -1406,7 +1438,7 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         if ((s = grad_exact_backward(tp, z, z2))) return s;
     } else {
         CK(launch_scatter(g_, zc_.as<double>(), n_num_, pos_.as<long long>(), 1.0, z, st_), "scatter z");
-        CK(launch_dot_gh(g_, z, gh_.as<double>(), prow(0, nt), nsbx_, nsby_, st_), "z.gh");
+        CK(launch_dot_gh(g_, z, gh_.as<double>(), prow(0, nt), nsbx_, nsby_, st_, segs_), "z.gh");
         launches_ += 2;
         if (tp.policy == FKADJ_CKPT_SQRT) CK(flush_range(0, nt, 1), "reduce z.gh");
         else if (nt % pwin_ == 0) CK(flush_rows(0, nt, nt + 1), "reduce z.gh");
@@ -1429,8 +1461,9 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
                          const double* fb) -> fkadj_status {
         const int nxt = 1 - cur_c;
         const double* fin = fb ? fb : (have_fcarry ? fc[cur_c] : nullptr);
-        if (adj_path_ != ADJ_SPLIT) {
-            // one launch: midpoint and the four stages (k_adj_fused); the
+        if (adj_path_ != ADJ_SPLIT && !segs_) {
+            // one launch: midpoint and the four stages (k_adj_fused, which
+            // writes its partials on the 16x16 lattice only); the
             // J(y) cache of the previous step in the ADJ_FUSED path
             const bool cache = adj_path_ == ADJ_FUSED;
             CK(prof_begin(K_ADJ), "profiling event");
@@ -1461,7 +1494,8 @@ fkadj_status Problem::grad_sequence(const TrajPlan& tp, bool exact, double** yT_
         CK(prof_begin(K_ADJ), "profiling event");
         CK(launch_adj_step(tk_[T_ADJ], P_, g_, z, z2, yb, yh_.as<double>(), ya, wc_.as<uint8_t>(),
                            gh_.as<double>(), prow(0, i - 1), nsbx_, st_, fault(),
-                           (carry && have_jcarry) ? jy[cur_c] : nullptr, jhc, carry ? jy[nxt] : nullptr),
+                           (carry && have_jcarry) ? jy[cur_c] : nullptr, jhc, carry ? jy[nxt] : nullptr, ty_[T_ADJ],
+                           segs_),
            "adjoint step");
         CK(prof_end(K_ADJ), "profiling event");
         launches_ += 2;

@@ -216,6 +216,10 @@ private:
     HermiteW hw_{};
     double dt_ = 0, alpha_ = 0, gamma_[3] = {0, 0, 0};
     int nt_ = 0, n_num_ = 0, device_ = 0, nsbx_ = 0, nsby_ = 0, nsb_ = 0;
+    // z.gh partials on the row-segment lattice (nsb_ = nsbx_ x nrows; the
+    // adjoint step's tiles then take balanced rows) instead of the 16x16 one
+    // (nsb_ = nsbx_ x nsby_); chosen by ensure_adjoint_work
+    bool segs_ = false;
     int tk_[4] = {0, 0, 0, 0};  // tile preset per kernel kind (TileKind)
     int tkf_ = 0;               // fused reference-adjoint preset (fused_shape)
     int adj_path_ = 0;          // AdjPath of the reference-mode backward step

@@ -229,6 +229,29 @@ __device__ __forceinline__ void subblock_sums(Term term, double* __restrict__ ro
     }
 }
 
+// The same on the lattice of 16-cell row segments (one partial per grid row
+// and 16 columns), for tiles of any height: half-warp h takes segment b of the
+// tile (rows x TX/16 segments, row-major), lane l of the half adds cell l, and
+// an xor butterfly over the 16 lanes leaves the sum in lane 0 in an order fixed
+// by the segment alone.  Every thread runs every round (the shuffles take the
+// whole warp).  One partial per segment goes to row[(i0 + r) * nsbx + j0/16 + sx].
+template <int TX, int NT, class Term>
+__device__ __forceinline__ void segment_sums(Term term, double* __restrict__ row, int i0, int j0, int nsbx,
+                                             int rows) {
+    constexpr int SX = TX / 16, NH = NT / 16;
+    const int l = threadIdx.x & 15, h = threadIdx.x >> 4;
+    const int nseg = SX * rows;
+    for (int b0 = 0; b0 < nseg; b0 += NH) {
+        const int b = b0 + h;
+        const bool on = b < nseg;
+        const int r = on ? b / SX : 0, sx = on ? b - r * SX : 0;
+        double s = on ? term(r, sx * 16 + l) : 0.0;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (on && l == 0) row[(long long)(i0 + r) * nsbx + (j0 / 16 + sx)] = s;
+    }
+}
+
 // ---------------------------------------------------------------- forward
 
 // One forward RK stage on the tile grown by E cells: k = f(src), then
@@ -579,14 +602,16 @@ __device__ __forceinline__ void adj_stage(const DevModel& P, const DevGrid& g, c
                                           const double* __restrict__ z0g, const uint8_t* __restrict__ wc,
                                           const double* __restrict__ ys, long long off, double cZ, double cD,
                                           double* __restrict__ out, const double* __restrict__ gh,
-                                          const double* __restrict__ jload, double* __restrict__ jstore) {
+                                          const double* __restrict__ jload, double* __restrict__ jstore,
+                                          int rows = TY) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
-    constexpr int W = TX + 2 * E, H = TY + 2 * E, N = W * H;
+    constexpr int W = TX + 2 * E;
     constexpr int IN = TX * TY;
+    const int N = W * (rows + 2 * E);
     // the stage update of cell (r, c) from its step-start value and k
     auto finish = [&](int r, int c, int s, long long o, double a, double b, double e, double ku, double kv,
                       double kw) {
-        const bool inner = (E == 0) || (r >= HALO && r < HALO + TY && c >= HALO && c < HALO + TX);
+        const bool inner = (E == 0) || (r >= HALO && r < HALO + rows && c >= HALO && c < HALO + TX);
         const int d = (r - HALO) * TX + (c - HALO);
         if (MODE == 2) {
             const double nu = (a + D[d]) + cD * ku;
@@ -721,27 +746,37 @@ __device__ __forceinline__ void adj_step_tile(const DevModel& P, const DevGrid& 
                                               const uint8_t* __restrict__ wc, const double* __restrict__ gh,
                                               double* __restrict__ row, int nsbx, const double* __restrict__ jb,
                                               const double* __restrict__ jh, double* __restrict__ ja, int tbx,
-                                              int tby, unsigned* fault = nullptr, uint32_t* phase = nullptr) {
+                                              int tby, unsigned* fault = nullptr, uint32_t* phase = nullptr,
+                                              int ty = TY, bool segments = false) {
     constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
     extern __shared__ double4 smem_raw[];
     double* A = reinterpret_cast<double*>(smem_raw);
     double* B = A + 3 * RN;
     double* D = B + 3 * RN;
-    const int i0 = tby * TY, j0 = tbx * TX;
+    // On the row-segment lattice a tile has ty <= TY rows, cut at the grid's
+    // edge; on the 16x16 sub-block lattice ty = TY and the tile keeps all TY
+    // rows (rows past the edge are NaN ring or padding and sum to 0).
+    const int i0 = tby * ty, j0 = tbx * TX;
+    const int rows = segments ? min(ty, g.nrows - i0) : TY;
     const long long off = (long long)i0 * g.ld + j0;
     const bool vec_ok = ((g.ld | j0) & 1) == 0;
-    if (!load_windows<RH, RW, NT, BULK>(A, z + off, nullptr, nullptr, g.ld, g.plane, vec_ok, RH, fault, nullptr,
-                                        nullptr, phase))
+    if (!load_windows<RH, RW, NT, BULK>(A, z + off, nullptr, nullptr, g.ld, g.plane, vec_ok, rows + 2 * HALO,
+                                        fault, nullptr, nullptr, phase))
         return;
     const double dt = P.dt;
     adj_stage<3, TX, TY, NT, 0, PF>(P, g, A, B, D, z, wc, yb, off, 0.5 * dt, 1.0 / 6.0 * dt, nullptr, gh, jb,
-                                    nullptr);
+                                    nullptr, rows);
     adj_stage<2, TX, TY, NT, 1, PF>(P, g, B, A, D, z, wc, yh, off, 0.5 * dt, 2.0 / 6.0 * dt, nullptr, gh, jh,
-                                    nullptr);
-    adj_stage<1, TX, TY, NT, 1, PF>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr);
-    adj_stage<0, TX, TY, NT, 2, PF>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, nullptr, ja);
+                                    nullptr, rows);
+    adj_stage<1, TX, TY, NT, 1, PF>(P, g, A, B, D, z, wc, yh, off, dt, 2.0 / 6.0 * dt, nullptr, gh, jh, nullptr,
+                                    rows);
+    adj_stage<0, TX, TY, NT, 2, PF>(P, g, B, A, D, z, wc, ya, off, 0.0, 1.0 / 6.0 * dt, zout, gh, nullptr, ja,
+                                    rows);
     __syncthreads();
-    subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
+    if (segments)
+        segment_sums<TX, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx, rows);
+    else
+        subblock_sums<TX, TY, NT>([&](int r, int c) { return D[r * TX + c]; }, row, i0, j0, nsbx);
 }
 
 template <int TX, int TY, int NT>
@@ -750,11 +785,12 @@ __global__ void __launch_bounds__(NT, min_blocks(TX, TY, NT))
                const double* __restrict__ yb, const double* __restrict__ yh, const double* __restrict__ ya,
                const uint8_t* __restrict__ wc, const double* __restrict__ gh, double* __restrict__ row, int nsbx,
                const double* __restrict__ jb, const double* __restrict__ jh, double* __restrict__ ja,
-               unsigned* fault) {
+               unsigned* fault, int ty, int segments) {
     pdl_enter();
     exp_table_init();
     adj_step_tile<TX, TY, NT, true, FKADJ_ADJ_PREFETCH != 0>(P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh,
-                                                             ja, blockIdx.x, blockIdx.y, fault);
+                                                             ja, blockIdx.x, blockIdx.y, fault, nullptr, ty,
+                                                             segments != 0);
 }
 
 // ------------------------------------------- fused reference-mode adjoint
@@ -1265,6 +1301,26 @@ __global__ void __launch_bounds__(32) k_dot_gh(DevGrid g, const double* __restri
         row, by * 16, bx * 16, nsbx);
 }
 
+// The same on the row-segment lattice (segment_sums' order): half-warp h of
+// block b takes segment 16 b + h of the grid (nseg = nsbx x nrows, row-major).
+__global__ void __launch_bounds__(256) k_dot_gh_segments(DevGrid g, const double* __restrict__ z,
+                                                         const double* __restrict__ gh, double* __restrict__ row,
+                                                         int nsbx, int nseg) {
+    const int l = threadIdx.x & 15;
+    const int b = blockIdx.x * 16 + (threadIdx.x >> 4);
+    const bool on = b < nseg;
+    const int r = on ? b / nsbx : 0, sx = on ? b - r * nsbx : 0;
+    double s = 0.0;
+    if (on) {
+        const long long o = (long long)(r + HALO) * g.ld + (sx * 16 + l + HALO);
+        const double t = z[o] * gh[o];
+        s = isnan(t) ? 0.0 : t;
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (on && l == 0) row[b] = s;
+}
+
 // out[row] = sum_k partial[row*ntiles + k], fixed order (one block per row).
 __global__ void k_sum_rows(const double* __restrict__ partial, int ntiles, double* __restrict__ out) {
     __shared__ double red[8];
@@ -1586,8 +1642,9 @@ static int wave_rows(K kernel, int nt, size_t smem, int tx, int ty, const DevGri
 int balanced_rows(int tile, int kind, const DevGrid& g) {
     int r = 0;
     DISPATCH(tile, {
-        r = kind == 0 ? wave_rows(k_fwd_step<TX, TY, NT>, NT, stencil_smem<TX, TY>(NT), TX, TY, g)
-                      : wave_rows(k_adj_mid<TX, TY, NT>, NT, mid_smem<TX, TY>(), TX, TY, g);
+        r = kind == 0   ? wave_rows(k_fwd_step<TX, TY, NT>, NT, stencil_smem<TX, TY>(NT), TX, TY, g)
+            : kind == 1 ? wave_rows(k_adj_mid<TX, TY, NT>, NT, mid_smem<TX, TY>(), TX, TY, g)
+                        : wave_rows(k_adj_step<TX, TY, NT>, NT, stencil_smem<TX, TY>(NT), TX, TY, g);
     });
     return r;
 }
@@ -1595,10 +1652,13 @@ int balanced_rows(int tile, int kind, const DevGrid& g) {
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
                             const double* gh, double* row, int nsbx, cudaStream_t st, unsigned* fault,
-                            const double* jb, const double* jh, double* ja) {
+                            const double* jb, const double* jh, double* ja, int ty, bool segments) {
     DISPATCH(tile, {
-        const cudaError_t e = launch_pdl(k_adj_step<TX, TY, NT>, tile_grid(g, TX, TY), NT, stencil_smem<TX, TY>(NT),
-                                         st, P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, fault);
+        // rows other than the preset's height only on the row-segment lattice
+        const int rows = (segments && ty > 0 && ty < TY) ? ty : TY;
+        const cudaError_t e = launch_pdl(k_adj_step<TX, TY, NT>, tile_grid(g, TX, rows), NT, stencil_smem<TX, TY>(NT),
+                                         st, P, g, z, zout, yb, yh, ya, wc, gh, row, nsbx, jb, jh, ja, fault, rows,
+                                         segments ? 1 : 0);
         if (e != cudaSuccess) return e;
     });
     return cudaGetLastError();
@@ -1680,8 +1740,13 @@ cudaError_t launch_batch_fused(int tile, const BatchInstance* d_inst, const Batc
 }
 
 cudaError_t launch_dot_gh(const DevGrid& g, const double* z, const double* gh, double* row, int nsbx, int nsby,
-                          cudaStream_t st) {
-    k_dot_gh<<<nsbx * nsby, 32, 0, st>>>(g, z, gh, row, nsbx);
+                          cudaStream_t st, bool segments) {
+    if (segments) {
+        const int nseg = nsbx * g.nrows;
+        k_dot_gh_segments<<<(nseg + 15) / 16, 256, 0, st>>>(g, z, gh, row, nsbx, nseg);
+    } else {
+        k_dot_gh<<<nsbx * nsby, 32, 0, st>>>(g, z, gh, row, nsbx);
+    }
     return cudaGetLastError();
 }
 

@@ -126,12 +126,15 @@ cudaError_t launch_fwd_step(int tile, const DevModel& P, const DevGrid& g, const
 // (on by default; the engine turns it off while it captures a graph).
 void set_launch_pdl(bool on);
 // Rows per tile that fit grid g into one wave of CTAs of preset `tile` for
-// kernel kind 0 (forward step) or 1 (adjoint midpoint); the preset's height
-// when it does not fit.
+// kernel kind 0 (forward step), 1 (adjoint midpoint) or 2 (adjoint step); the
+// preset's height when it does not fit.
 int balanced_rows(int tile, int kind, const DevGrid& g);
 // The z.gh style reductions write one partial per 16x16 sub-block of the
 // grid's lattice (nsbx x nsby, covering the 64-padded grid); sub-blocks no
-// tile covers are never written and must be zero.
+// tile covers are never written and must be zero.  The reference-mode adjoint
+// step and launch_dot_gh can instead write one partial per 16-cell row segment
+// (segments = true: nsbx x nrows partials per row of results), which lets the
+// step's tiles take any number of rows.
 void subblock_lattice(const DevGrid& g, int* nsbx, int* nsby);
 cudaError_t launch_adj_exact(int tile, const DevModel& P, const DevGrid& g, const double* lam, double* lamout,
                              const double* y, const double* stages, const uint8_t* wc, const double* gh,
@@ -142,10 +145,14 @@ cudaError_t launch_adj_mid(int tile, const DevModel& P, const DevGrid& g, const 
                            double* jh = nullptr, int ty = 0, const double* fa = nullptr);
 // jb: cached J(y_i) (null = evaluate), jh: cached J(yh) (null = evaluate),
 // ja: where J(y_{i-1}) is stored for the next step (null = not kept).
+// segments: z.gh partials on the row-segment lattice, with ty rows per tile
+// (0 = the preset's height); otherwise on the 16x16 lattice with the preset's
+// height.
 cudaError_t launch_adj_step(int tile, const DevModel& P, const DevGrid& g, const double* z, double* zout,
                             const double* yb, const double* yh, const double* ya, const uint8_t* wc,
                             const double* gh, double* row, int nsbx, cudaStream_t st, unsigned* fault,
-                            const double* jb = nullptr, const double* jh = nullptr, double* ja = nullptr);
+                            const double* jb = nullptr, const double* jh = nullptr, double* ja = nullptr,
+                            int ty = 0, bool segments = false);
 // Fused reference-adjoint step (k_adj_mid and k_adj_step in one launch):
 // z -> zout over step [t_{i-1}, t_i] with ya = y_{i-1}, yb = y_i; fa, fb =
 // f(ya, Et[i-1]), f(yb, Et[i]) where kept or carried (null = evaluated), fout
@@ -160,7 +167,7 @@ cudaError_t launch_adj_fused(int tile, const DevModel& P, const DevGrid& g, cons
                              const uint8_t* wc, const double* gh, const EStep& E, const HermiteW& hw, double* row,
                              int nsbx, const double* jb, double* ja, cudaStream_t st, unsigned* fault);
 cudaError_t launch_dot_gh(const DevGrid& g, const double* z, const double* gh, double* row, int nsbx, int nsby,
-                          cudaStream_t st);
+                          cudaStream_t st, bool segments = false);
 cudaError_t launch_sum_rows(const double* partial, int rows, int ntiles, double* out, cudaStream_t st);
 cudaError_t launch_scatter(const DevGrid& g, const double* yc, int n_num, const long long* pos, double scale,
                            double* y, cudaStream_t st);

@@ -239,3 +239,20 @@ def test_auto_store_takes_the_schedule_that_recomputes_less(mode):
         assert plan["recompute_steps"] == {"sqrt": 119, "binomial": 32 if states == 100 else 102}[want]
         assert np.array_equal(r["gradE"], full[0])
         assert r["Lcost"] == full[1]
+
+
+@pytest.mark.parametrize("ckpt", [_lib.CKPT_SQRT, _lib.CKPT_FULL])
+def test_zgh_row_segment_lattice_agrees_with_16x16_lattice(monkeypatch, ckpt):
+    """The reference-mode step's z.gh partials on 16-cell row segments (tiles of
+    any height, the default where 64x32 tiles fit one wave) and on 16x16
+    sub-blocks (FKADJ_ZGH_SEGMENTS=0) sum the same terms in two fixed orders:
+    gradients within 1e-13, objectives equal; on a ragged grid (rows and
+    columns not multiples of 16) and a horizon whose rows span several windows."""
+    inst = _inst(90, 700, seed=41, ncols=75, objective="gradient", alpha=0.1)
+    args = (inst.Et, inst.dt, inst.nt, inst.y0, inst.active_index, inst.ncols, inst.nrows, inst.ghost, inst.gamma,
+            inst.S, inst.alpha)
+    seg = api.fk_grad_Et(*args, params=inst.params, opts=api.options(ckpt_policy=ckpt))
+    monkeypatch.setenv("FKADJ_ZGH_SEGMENTS", "0")
+    blk = api.fk_grad_Et(*args, params=inst.params, opts=api.options(ckpt_policy=ckpt))
+    assert np.linalg.norm(seg[0] - blk[0]) <= 1e-13 * np.linalg.norm(blk[0])
+    assert seg[1] == blk[1]
