@@ -450,6 +450,12 @@ def run_ours(args):
     d2h = (inst.nt + 1) * 8 + 3 * 8
     eopts = api.options(ckpt_policy=ckpt, device=local, tile=args.tile, grad_mode=gmode)
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    # one untimed call first, as every timed loop here has warm-up steps: a
+    # process's first drop-in call also grows the one-shot memory pool and the
+    # pinned staging (measured 50-270 ms more than the steady calls)
+    api.fk_grad_Et(Et_h, inst.dt, inst.nt, y0_h, ai_h, inst.ncols, inst.nrows, gh_h, inst.gamma, S, inst.alpha,
+                   params=inst.params, opts=eopts)
+    torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -459,7 +465,8 @@ def run_ours(args):
     e2e_s = gmax(time.perf_counter() - t0)
     e2e = {"value": replica_value(world, e2e_steps, e2e_s * 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-           "path": "fkadj_grad (drop-in for fk_grad_Et_comp), one call per gradient incl. device setup"}
+           "path": "fkadj_grad (drop-in for fk_grad_Et_comp), one call per gradient incl. device setup, "
+                   "after one untimed call"}
 
     # the metric's second half: served p50/p99 against plain solves, and the
     # batched uneven instances, at a stated scale-down of their workloads
