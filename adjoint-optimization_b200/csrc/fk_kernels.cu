@@ -506,7 +506,7 @@ __device__ __forceinline__ void adj_mid_tile(const DevModel& P, const DevGrid& g
             };
             auto fetch = [&](int r, int c, Ops& x) {
                 const long long o = off + (long long)r * g.ld + c;
-                x.gg = __ldg(gh + o);
+                if (!fa || !fin) x.gg = __ldg(gh + o);  // only an evaluated f needs E gh
                 if (fa) x.a0[0] = __ldg(fa + o), x.a0[1] = __ldg(fa + g.plane + o), x.a0[2] = __ldg(fa + 2 * g.plane + o);
                 if (fin)
                     x.a1[0] = __ldg(fin + o), x.a1[1] = __ldg(fin + g.plane + o), x.a1[2] = __ldg(fin + 2 * g.plane + o);
