@@ -958,20 +958,19 @@ fkadj_status Problem::ensure_adjoint_work(bool all_rows) {
         const int c = traj_plan_.stride;
         win = std::min(per_group, c >= kPartialWindow ? c : c * (kPartialWindow / c));
     }
-    // Lattice of the partials.  Row segments (16 times as many partials as
-    // 16x16 sub-blocks) where the reference-mode split step reduces windowed
-    // partials, the window shrunk, in whole segments under a sqrt store, until
-    // it holds no more than the full rows of 16x16 partials that
-    // estimate_bytes counts; the 16x16 lattice for the exact mode, the fused
-    // step, the batch engine's all-rows buffers, where no window fits, or under
-    // FKADJ_ZGH_SEGMENTS=0.
-    // The choice depends on the grid, the horizon and the device only, never on
-    // the store, so that every store gives the same bits: row segments need
-    // room for one segment of rows of the sqrt store (whichever store runs),
-    // and pay only where 64x32 tiles fit the grid into one wave of CTAs, one
-    // per SM (512 x 512 and below): there tiles of any height make the wave
-    // full (512^2 x 2000 gradient 132.0 -> 129.4 ms), while at 2048 x 2048,
-    // 14 waves, the 16-fold partials cost 1.4 %.
+    // Lattice of the partials: 16-cell row segments (16 times as many partials
+    // as 16x16 sub-blocks; the adjoint step's tiles may then take any height)
+    // for the reference-mode split step with windowed partials, where 64x32
+    // tiles fit the grid into one wave of CTAs, one per SM (512 x 512 and
+    // below: tiles of the one-wave height fill the wave, 512^2 x 2000 gradient
+    // 132.0 -> 129.4 ms; at 2048 x 2048, 14 waves, the 16-fold partials cost
+    // 1.4 %), and where a window of one sqrt segment of rows fits within the
+    // full rows of 16x16 partials that estimate_bytes counts; the window then
+    // shrinks, in whole segments under a sqrt store, to fit there.  The choice
+    // depends on the grid, the horizon and the device only, never on the store,
+    // so that every store gives the same bits.  The 16x16 lattice otherwise:
+    // the exact mode, the fused step, the batch engine's all-rows buffers, and
+    // under FKADJ_ZGH_SEGMENTS=0.
     const size_t nsb16 = (size_t)nsbx_ * (size_t)nsby_, nsbseg = (size_t)nsbx_ * (size_t)g_.nrows;
     const size_t fit = prow * (nsb16 + 1) / nsbseg;  // rows of segment partials within that count
     const int c_sqrt = std::max(2, (int)std::ceil(std::sqrt((double)nt_)));  // plan_trajectory's stride

@@ -124,7 +124,11 @@ public:
     void set_tile(int kind, int t) { tk_[kind] = t; }
     // rows per tile in use for a kernel kind (the preset's height, or fewer
     // when the autotuner found a one-wave split faster)
-    int tile_rows(int kind) const { return ty_[kind] > 0 ? ty_[kind] : tile_shape(tk_[kind]).ty; }
+    // rows per tile of a kernel kind as launched (the adjoint step takes its
+    // rows on the row-segment lattice only)
+    int tile_rows(int kind) const {
+        return ty_[kind] > 0 && (kind != T_ADJ || segs_) ? ty_[kind] : tile_shape(tk_[kind]).ty;
+    }
     // Times every tile preset of every kernel kind on the current initial
     // state (a few launches each) and keeps the fastest per kind.  Results do
     // not depend on the choice (fixed-order reductions).
